@@ -1,0 +1,25 @@
+"""gf2_b200: B200-native (sm_100a) batched LDPC encoder / decoder.
+
+A drop-in for the belief-propagation path of erankavija/gf2's gf2-coding crate.
+The compute runs in libgf2cuda.so (hand-written CUDA for sm_100a) behind the C
+ABI of include/gf2cuda.h; this package is the host-side mirror of the
+reference's Rust API over that ABI.
+"""
+from . import _capi
+from .ldpc import (AwgnChannel, BpskModulator, CirculantMatrix, CodeRate, DecoderResult, FrameSize, Llr,
+                   LdpcCode, LdpcDecoder, LdpcEncoder, QuasiCyclicLdpc, awgn_frames, pack_bits, sigma2_from_ebn0,
+                   unpack_bits, words)
+
+ALGO_MINSUM = _capi.ALGO_MINSUM
+ALGO_SPA = _capi.ALGO_SPA
+ALGO_NMS = _capi.ALGO_NMS
+SCHED_FLOODING = _capi.SCHED_FLOODING
+SCHED_LAYERED = _capi.SCHED_LAYERED
+MSG_F32 = _capi.MSG_F32
+MSG_F16 = _capi.MSG_F16
+Gf2cError = _capi.Gf2cError
+
+__all__ = ["AwgnChannel", "BpskModulator", "CirculantMatrix", "CodeRate", "DecoderResult", "FrameSize", "Llr",
+           "LdpcCode", "LdpcDecoder", "LdpcEncoder", "QuasiCyclicLdpc", "awgn_frames", "pack_bits",
+           "sigma2_from_ebn0", "unpack_bits", "words", "ALGO_MINSUM", "ALGO_SPA", "ALGO_NMS", "SCHED_FLOODING",
+           "SCHED_LAYERED", "MSG_F32", "MSG_F16", "Gf2cError"]

@@ -1,0 +1,100 @@
+"""ctypes binding of libgf2cuda.so (the C ABI declared in include/gf2cuda.h).
+
+There is no fallback: if the shared library is missing or fails to load,
+importing the binding raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgf2cuda.so")
+
+OK = 0
+ERR_INVALID_ARG = 1
+ERR_CUDA = 2
+ERR_UNSUPPORTED = 3
+ERR_NOMEM = 4
+ERR_RANK = 5
+ERR_KERNEL = 6
+MEM_HOST = 0
+MEM_DEVICE = 1
+ALGO_MINSUM = 0
+ALGO_SPA = 1
+ALGO_NMS = 2
+SCHED_FLOODING = 0
+SCHED_LAYERED = 1
+MSG_F32 = 0
+MSG_F16 = 1
+
+# Every symbol the header declares, for the load / export check.
+EXPORTS = [
+    "gf2c_decoder_opts_default", "gf2c_last_error", "gf2c_version",
+    "gf2c_code_create_dvbt2", "gf2c_code_create_qc", "gf2c_code_create_edges",
+    "gf2c_code_destroy", "gf2c_code_dims", "gf2c_code_csr", "gf2c_syndrome_batch",
+    "gf2c_encode_batch", "gf2c_channel_awgn", "gf2c_sigma2_from_ebn0",
+    "gf2c_decoder_create", "gf2c_decoder_create_multi", "gf2c_decoder_destroy",
+    "gf2c_decode_batch", "gf2c_decode_mixed", "gf2c_decoder_last_launches",
+]
+
+
+class DecoderOpts(ctypes.Structure):
+    _fields_ = [
+        ("algorithm", ctypes.c_int32),
+        ("schedule", ctypes.c_int32),
+        ("msg_dtype", ctypes.c_int32),
+        ("early_stop", ctypes.c_int32),
+        ("nms_alpha", ctypes.POINTER(ctypes.c_float)),
+        ("nms_beta", ctypes.POINTER(ctypes.c_float)),
+        ("nms_iters", ctypes.c_int32),
+        ("threads_per_block", ctypes.c_int32),
+        ("blocks_per_sm", ctypes.c_int32),
+    ]
+
+
+class Gf2cError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"gf2cuda error {code}: {msg}")
+        self.code = code
+
+
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+_u64 = ctypes.c_uint64
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python gf2_b200/build.py`")
+    L = ctypes.CDLL(LIB_PATH)
+    L.gf2c_last_error.restype = ctypes.c_char_p
+    L.gf2c_version.restype = ctypes.c_char_p
+    L.gf2c_decoder_opts_default.argtypes = [ctypes.POINTER(DecoderOpts)]
+    L.gf2c_decoder_opts_default.restype = None
+    L.gf2c_code_create_dvbt2.argtypes = [_i32, _i32, ctypes.POINTER(_vp)]
+    L.gf2c_code_create_qc.argtypes = [_vp, _i32, _i32, _i32, ctypes.POINTER(_vp)]
+    L.gf2c_code_create_edges.argtypes = [_i64, _i64, _vp, _i64, ctypes.POINTER(_vp)]
+    L.gf2c_code_destroy.argtypes = [_vp]
+    L.gf2c_code_dims.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
+    L.gf2c_code_csr.argtypes = [_vp, _vp, _vp]
+    L.gf2c_syndrome_batch.argtypes = [_vp, _vp, _i64, _vp, _vp, _i32, _vp]
+    L.gf2c_encode_batch.argtypes = [_vp, _vp, _i64, _vp, _i32, _vp]
+    L.gf2c_channel_awgn.argtypes = [_vp, _u64, _u64, _i64, _vp, _vp, _vp, _vp, _i32, _vp]
+    L.gf2c_sigma2_from_ebn0.argtypes = [ctypes.c_double, ctypes.c_double]
+    L.gf2c_sigma2_from_ebn0.restype = ctypes.c_double
+    L.gf2c_decoder_create.argtypes = [_vp, ctypes.POINTER(DecoderOpts), ctypes.POINTER(_vp)]
+    L.gf2c_decoder_create_multi.argtypes = [_vp, _i32, ctypes.POINTER(DecoderOpts), ctypes.POINTER(_vp)]
+    L.gf2c_decoder_destroy.argtypes = [_vp]
+    L.gf2c_decode_batch.argtypes = [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _vp]
+    L.gf2c_decode_mixed.argtypes = [_vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _vp]
+    L.gf2c_decoder_last_launches.argtypes = [_vp, ctypes.POINTER(_i32)]
+    return L
+
+
+lib = _load()
+
+
+def check(rc):
+    if rc != OK:
+        raise Gf2cError(rc, lib.gf2c_last_error().decode())
+    return rc

@@ -1,0 +1,551 @@
+// gf2cuda C ABI implementation: argument validation, device workspace, host
+// staging, launch shapes and CUDA-graph replay.  Every entry point returns a
+// status code; nothing aborts.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <tuple>
+
+#include "internal.h"
+
+namespace gf2c {
+
+static thread_local std::string g_error;
+
+int set_error(int code, const std::string& msg) {
+  g_error = msg;
+  return code;
+}
+
+int cuda_error(cudaError_t e, const char* what) {
+  g_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return GF2C_ERR_CUDA;
+}
+
+// Device buffer that only grows.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t need) {
+    if (need <= bytes) return GF2C_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t sz = std::max(need, (size_t)256);
+    cudaError_t e = cudaMalloc(&p, sz);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMalloc");
+    bytes = sz;
+    return GF2C_OK;
+  }
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+}  // namespace gf2c
+
+using namespace gf2c;
+
+struct GraphKey {
+  std::vector<uintptr_t> v;
+  bool operator<(const GraphKey& o) const { return v < o.v; }
+};
+
+struct gf2c_decoder {
+  std::vector<const gf2c_code*> codes;
+  gf2c_decoder_opts opts{};
+  int dev = 0;
+  DevBuf d_codes;
+  int max_n = 0, max_words_k = 0, max_e_slots = 0, max_dc = 0, max_nchk = 0;
+  int dcmax = 0, threads = 0, grid = 0, bitmap_words = 0, smem_app_floats = 0;
+  size_t smem = 0;
+  long long work_stride = 0, app_offset = 0;
+  DevBuf work, queue, status, alpha, beta;
+  int nms_iters = 0, nms_L = 0;
+  // staging for host-memory calls
+  DevBuf s_llr, s_msg, s_it, s_cv, s_so, s_bel, s_off1, s_off2, s_cid, s_mit;
+  int last_launches = 0;
+  std::map<GraphKey, cudaGraphExec_t> graphs;
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  ~gf2c_decoder() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    if (gstream) {
+      cudaStreamSynchronize(gstream);
+      cudaStreamDestroy(gstream);
+    }
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
+  }
+};
+
+extern "C" {
+
+const char* gf2c_last_error(void) { return g_error.c_str(); }
+const char* gf2c_version(void) { return "gf2cuda 0.1 (sm_100a)"; }
+
+void gf2c_decoder_opts_default(gf2c_decoder_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->algorithm = GF2C_ALGO_MINSUM;
+  o->schedule = GF2C_SCHED_FLOODING;
+  o->msg_dtype = GF2C_MSG_F32;
+  o->early_stop = 1;
+}
+
+double gf2c_sigma2_from_ebn0(double ebn0_db, double rate) {
+  return 1.0 / (2.0 * rate * std::pow(10.0, ebn0_db / 10.0));
+}
+
+static int make_code(gf2c_code** out, std::unique_ptr<HostCode> h) {
+  gf2c_code* c = new (std::nothrow) gf2c_code();
+  if (!c) return set_error(GF2C_ERR_NOMEM, "out of host memory");
+  c->h = std::move(h);
+  *out = c;
+  return GF2C_OK;
+}
+
+int gf2c_code_create_dvbt2(int32_t frame_size, int32_t rate, gf2c_code** out) {
+  if (!out) return set_error(GF2C_ERR_INVALID_ARG, "out is NULL");
+  auto h = std::make_unique<HostCode>();
+  int rc = build_dvbt2(frame_size, rate, *h);
+  if (rc) return rc;
+  return make_code(out, std::move(h));
+}
+
+int gf2c_code_create_qc(const int32_t* base, int32_t mb, int32_t nb, int32_t z, gf2c_code** out) {
+  if (!out) return set_error(GF2C_ERR_INVALID_ARG, "out is NULL");
+  auto h = std::make_unique<HostCode>();
+  int rc = build_qc(base, mb, nb, z, *h);
+  if (rc) return rc;
+  return make_code(out, std::move(h));
+}
+
+int gf2c_code_create_edges(int64_t m, int64_t n, const int64_t* pairs, int64_t count, gf2c_code** out) {
+  if (!out) return set_error(GF2C_ERR_INVALID_ARG, "out is NULL");
+  auto h = std::make_unique<HostCode>();
+  int rc = build_edges(m, n, pairs, count, *h);
+  if (rc) return rc;
+  return make_code(out, std::move(h));
+}
+
+int gf2c_code_destroy(gf2c_code* code) {
+  delete code;
+  return GF2C_OK;
+}
+
+int gf2c_code_dims(const gf2c_code* code, int64_t* n, int64_t* m, int64_t* k, int64_t* nnz,
+                   int32_t* layers) {
+  if (!code) return set_error(GF2C_ERR_INVALID_ARG, "code is NULL");
+  const HostCode& h = *code->h;
+  if (n) *n = h.n;
+  if (m) *m = h.m;
+  if (k) *k = h.k;
+  if (nnz) *nnz = (int64_t)h.row_idx.size();
+  if (layers) *layers = h.layered_ok ? (int32_t)h.cg.size() : 0;
+  return GF2C_OK;
+}
+
+int gf2c_code_csr(const gf2c_code* code, int64_t* indptr, int64_t* indices) {
+  if (!code || !indptr || !indices) return set_error(GF2C_ERR_INVALID_ARG, "NULL argument");
+  const HostCode& h = *code->h;
+  std::memcpy(indptr, h.row_ptr.data(), sizeof(int64_t) * h.row_ptr.size());
+  if (!h.row_idx.empty()) std::memcpy(indices, h.row_idx.data(), sizeof(int64_t) * h.row_idx.size());
+  return GF2C_OK;
+}
+
+// ---------------------------------------------------------------------------
+// helpers for host / device argument handling
+// ---------------------------------------------------------------------------
+static int check_mem(int32_t mem) {
+  if (mem != GF2C_MEM_HOST && mem != GF2C_MEM_DEVICE)
+    return set_error(GF2C_ERR_INVALID_ARG, "mem must be GF2C_MEM_HOST or GF2C_MEM_DEVICE");
+  return GF2C_OK;
+}
+
+static int ensure_code_on_device(const gf2c_code* code) {
+  return upload_code(*code->h);
+}
+
+// One DevCode on the device for single-code kernels (kept in the HostCode).
+static int code_dev_struct(const gf2c_code* code, DevBuf& buf) {
+  int rc = ensure_code_on_device(code);
+  if (rc) return rc;
+  if ((rc = buf.ensure(sizeof(DevCode)))) return rc;
+  GF2C_CUDA(cudaMemcpy(buf.p, &code->h->dev, sizeof(DevCode), cudaMemcpyHostToDevice));
+  return GF2C_OK;
+}
+
+struct CodeOps {
+  DevBuf dcode, in, out, aux, aux2;
+};
+static thread_local CodeOps g_ops;
+
+int gf2c_syndrome_batch(const gf2c_code* code, const uint64_t* cw_bits, int64_t frames,
+                        uint64_t* synd_bits, int32_t* weight, int32_t mem, void* stream) {
+  if (!code || frames < 0 || (frames > 0 && !cw_bits)) return set_error(GF2C_ERR_INVALID_ARG, "bad arguments");
+  int rc = check_mem(mem);
+  if (rc || frames == 0) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = code_dev_struct(code, g_ops.dcode))) return rc;
+  const DevCode& h = code->h->dev;
+  if (mem == GF2C_MEM_DEVICE)
+    return launch_syndrome((const DevCode*)g_ops.dcode.p, h, cw_bits, frames, synd_bits, weight, st);
+  size_t bin = (size_t)frames * h.words_n * 8, bs = (size_t)frames * h.words_m * 8, bw = (size_t)frames * 4;
+  if ((rc = g_ops.in.ensure(bin)) || (rc = g_ops.out.ensure(bs)) || (rc = g_ops.aux.ensure(bw))) return rc;
+  GF2C_CUDA(cudaMemcpyAsync(g_ops.in.p, cw_bits, bin, cudaMemcpyHostToDevice, st));
+  if ((rc = launch_syndrome((const DevCode*)g_ops.dcode.p, h, (const uint64_t*)g_ops.in.p, frames,
+                            (uint64_t*)g_ops.out.p, (int32_t*)g_ops.aux.p, st)))
+    return rc;
+  if (synd_bits) GF2C_CUDA(cudaMemcpyAsync(synd_bits, g_ops.out.p, bs, cudaMemcpyDeviceToHost, st));
+  if (weight) GF2C_CUDA(cudaMemcpyAsync(weight, g_ops.aux.p, bw, cudaMemcpyDeviceToHost, st));
+  GF2C_CUDA(cudaStreamSynchronize(st));
+  return GF2C_OK;
+}
+
+int gf2c_encode_batch(const gf2c_code* code, const uint64_t* msg_bits, int64_t frames, uint64_t* cw_bits,
+                      int32_t mem, void* stream) {
+  if (!code || frames < 0 || (frames > 0 && (!msg_bits || !cw_bits)))
+    return set_error(GF2C_ERR_INVALID_ARG, "bad arguments");
+  int rc = check_mem(mem);
+  if (rc || frames == 0) return rc;
+  if ((rc = prepare_encoder(*code->h))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = code_dev_struct(code, g_ops.dcode))) return rc;
+  const DevCode& h = code->h->dev;
+  if (mem == GF2C_MEM_DEVICE) return launch_encode((const DevCode*)g_ops.dcode.p, h, msg_bits, frames, cw_bits, st);
+  size_t bin = (size_t)frames * h.words_k * 8, bout = (size_t)frames * h.words_n * 8;
+  if ((rc = g_ops.in.ensure(bin)) || (rc = g_ops.out.ensure(bout))) return rc;
+  GF2C_CUDA(cudaMemcpyAsync(g_ops.in.p, msg_bits, bin, cudaMemcpyHostToDevice, st));
+  if ((rc = launch_encode((const DevCode*)g_ops.dcode.p, h, (const uint64_t*)g_ops.in.p, frames,
+                          (uint64_t*)g_ops.out.p, st)))
+    return rc;
+  GF2C_CUDA(cudaMemcpyAsync(cw_bits, g_ops.out.p, bout, cudaMemcpyDeviceToHost, st));
+  GF2C_CUDA(cudaStreamSynchronize(st));
+  return GF2C_OK;
+}
+
+int gf2c_channel_awgn(const gf2c_code* code, uint64_t seed, uint64_t frame0, int64_t frames,
+                      const double* sigma2, uint64_t* info_bits, uint64_t* cw_bits, float* llr,
+                      int32_t mem, void* stream) {
+  if (!code || frames < 0 || (frames > 0 && !sigma2)) return set_error(GF2C_ERR_INVALID_ARG, "bad arguments");
+  int rc = check_mem(mem);
+  if (rc || frames == 0) return rc;
+  if (mem == GF2C_MEM_HOST)
+    for (int64_t f = 0; f < frames; f++)
+      if (!(sigma2[f] > 0.0) || !std::isfinite(sigma2[f]))
+        return set_error(GF2C_ERR_INVALID_ARG, "sigma2 must be positive and finite");
+  if ((rc = prepare_encoder(*code->h))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = code_dev_struct(code, g_ops.dcode))) return rc;
+  const DevCode& h = code->h->dev;
+  if (mem == GF2C_MEM_DEVICE)
+    return launch_channel((const DevCode*)g_ops.dcode.p, h, seed, frame0, frames, sigma2, info_bits, cw_bits,
+                          llr, st);
+  size_t bi = (size_t)frames * h.words_k * 8, bc = (size_t)frames * h.words_n * 8,
+         bl = (size_t)frames * h.n * 4, bs = (size_t)frames * 8;
+  if ((rc = g_ops.in.ensure(bs)) || (rc = g_ops.out.ensure(bl)) || (rc = g_ops.aux.ensure(bi)) ||
+      (rc = g_ops.aux2.ensure(bc)))
+    return rc;
+  GF2C_CUDA(cudaMemcpyAsync(g_ops.in.p, sigma2, bs, cudaMemcpyHostToDevice, st));
+  if ((rc = launch_channel((const DevCode*)g_ops.dcode.p, h, seed, frame0, frames, (const double*)g_ops.in.p,
+                           info_bits ? (uint64_t*)g_ops.aux.p : nullptr,
+                           cw_bits ? (uint64_t*)g_ops.aux2.p : nullptr, llr ? (float*)g_ops.out.p : nullptr, st)))
+    return rc;
+  if (info_bits) GF2C_CUDA(cudaMemcpyAsync(info_bits, g_ops.aux.p, bi, cudaMemcpyDeviceToHost, st));
+  if (cw_bits) GF2C_CUDA(cudaMemcpyAsync(cw_bits, g_ops.aux2.p, bc, cudaMemcpyDeviceToHost, st));
+  if (llr) GF2C_CUDA(cudaMemcpyAsync(llr, g_ops.out.p, bl, cudaMemcpyDeviceToHost, st));
+  GF2C_CUDA(cudaStreamSynchronize(st));
+  return GF2C_OK;
+}
+
+// ---------------------------------------------------------------------------
+// decoder
+// ---------------------------------------------------------------------------
+static const int kSmemBudget = 200 * 1024;
+
+int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, const gf2c_decoder_opts* opts,
+                              gf2c_decoder** out) {
+  if (!out || !codes || ncodes <= 0) return set_error(GF2C_ERR_INVALID_ARG, "bad arguments");
+  *out = nullptr;
+  for (int i = 0; i < ncodes; i++)
+    if (!codes[i]) return set_error(GF2C_ERR_INVALID_ARG, "NULL code handle");
+  gf2c_decoder_opts o;
+  if (opts) o = *opts;
+  else gf2c_decoder_opts_default(&o);
+  if (o.algorithm < 0 || o.algorithm > 2 || o.schedule < 0 || o.schedule > 1 || o.msg_dtype < 0 ||
+      o.msg_dtype > 1 || o.threads_per_block < 0 || o.threads_per_block > 1024 || o.blocks_per_sm < 0 ||
+      (o.threads_per_block % 32) != 0)
+    return set_error(GF2C_ERR_INVALID_ARG, "invalid decoder options");
+  std::unique_ptr<gf2c_decoder> d(new (std::nothrow) gf2c_decoder());
+  if (!d) return set_error(GF2C_ERR_NOMEM, "out of host memory");
+  d->opts = o;
+  d->opts.nms_alpha = nullptr;
+  d->opts.nms_beta = nullptr;
+  GF2C_CUDA(cudaGetDevice(&d->dev));
+  std::vector<DevCode> dc;
+  for (int i = 0; i < ncodes; i++) {
+    if (!codes[i]) return set_error(GF2C_ERR_INVALID_ARG, "NULL code handle");
+    const HostCode& h = *codes[i]->h;
+    if (o.schedule == GF2C_SCHED_LAYERED && !h.layered_ok)
+      return set_error(GF2C_ERR_UNSUPPORTED, "layered schedule needs a QC or DVB-T2 code with Z <= 1024");
+    int rc = ensure_code_on_device(codes[i]);
+    if (rc) return rc;
+    d->codes.push_back(codes[i]);
+    dc.push_back(h.dev);
+    d->max_n = std::max(d->max_n, (int)h.n);
+    d->max_words_k = std::max(d->max_words_k, (int)((h.k + 63) / 64));
+    d->max_e_slots = std::max(d->max_e_slots, h.e_slots);
+    d->max_dc = std::max(d->max_dc, h.max_dc);
+    d->max_nchk = std::max(d->max_nchk, h.max_nchk);
+  }
+  d->dcmax = decode_dcmax_bucket(d->max_dc);
+  if (d->dcmax < 0) return set_error(GF2C_ERR_UNSUPPORTED, "check degree above 64");
+  int rc = d->d_codes.ensure(sizeof(DevCode) * dc.size());
+  if (rc) return rc;
+  GF2C_CUDA(cudaMemcpy(d->d_codes.p, dc.data(), sizeof(DevCode) * dc.size(), cudaMemcpyHostToDevice));
+
+  // NMS weights
+  if (o.algorithm == GF2C_ALGO_NMS) {
+    if (!opts || !opts->nms_alpha || !opts->nms_beta || opts->nms_iters <= 0)
+      return set_error(GF2C_ERR_INVALID_ARG, "NMS needs nms_alpha, nms_beta and nms_iters > 0");
+    const HostCode& h0 = *codes[0]->h;
+    d->nms_L = h0.layered_ok ? (int)h0.cg.size() : 1;
+    d->nms_iters = opts->nms_iters;
+    size_t nb = sizeof(float) * (size_t)d->nms_iters * d->nms_L;
+    for (size_t i = 0; i < (size_t)d->nms_iters * d->nms_L; i++)
+      if (!std::isfinite(opts->nms_alpha[i]) || !std::isfinite(opts->nms_beta[i]))
+        return set_error(GF2C_ERR_INVALID_ARG, "NMS weights must be finite");
+    if ((rc = d->alpha.ensure(nb)) || (rc = d->beta.ensure(nb))) return rc;
+    GF2C_CUDA(cudaMemcpy(d->alpha.p, opts->nms_alpha, nb, cudaMemcpyHostToDevice));
+    GF2C_CUDA(cudaMemcpy(d->beta.p, opts->nms_beta, nb, cudaMemcpyHostToDevice));
+  }
+
+  // launch shape
+  int sms = 148;
+  GF2C_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->dev));
+  int threads = o.threads_per_block;
+  if (threads == 0) threads = (o.schedule == GF2C_SCHED_LAYERED) ? ((d->max_nchk + 31) / 32) * 32 : 512;
+  if (o.schedule == GF2C_SCHED_LAYERED && threads < d->max_nchk)
+    return set_error(GF2C_ERR_INVALID_ARG, "layered schedule needs threads_per_block >= row group size");
+  threads = std::max(threads, 32);
+  d->threads = threads;
+  d->bitmap_words = (d->max_n + 31) / 32;
+  const int app_floats = d->max_n;
+  size_t bm = decode_smem_bytes(0, d->bitmap_words);
+  d->smem_app_floats = (bm + (size_t)app_floats * 4 <= (size_t)kSmemBudget) ? app_floats : 0;
+  // a mixed batch may still keep its shorter codes in shared memory
+  if (d->smem_app_floats == 0) {
+    int best = 0;
+    for (auto* c : d->codes)
+      if (bm + (size_t)c->h->n * 4 <= (size_t)kSmemBudget) best = std::max(best, (int)c->h->n);
+    d->smem_app_floats = best;
+  }
+  d->smem = decode_smem_bytes(d->smem_app_floats, d->bitmap_words);
+  const size_t msg_bytes = o.msg_dtype == GF2C_MSG_F16 ? 2 : 4;
+  const long long c2v_bytes = (((long long)d->max_e_slots * msg_bytes) + 255) / 256 * 256;
+  d->app_offset = c2v_bytes;
+  const bool need_gapp = d->max_n > d->smem_app_floats;
+  d->work_stride = c2v_bytes + (need_gapp ? ((long long)d->max_n * 4 + 255) / 256 * 256 : 0);
+  int occ = 0;
+  if ((rc = prepare_decode(o.algorithm, o.msg_dtype, o.schedule, d->dcmax, d->smem, threads, &occ))) return rc;
+  if (occ <= 0) return set_error(GF2C_ERR_UNSUPPORTED, "decode kernel does not fit on an SM with this shape");
+  int bps = o.blocks_per_sm ? std::min(o.blocks_per_sm, occ) : occ;
+  d->grid = sms * bps;
+  if ((rc = d->work.ensure((size_t)d->work_stride * d->grid))) return rc;
+  if ((rc = d->queue.ensure(64)) || (rc = d->status.ensure(64))) return rc;
+  GF2C_CUDA(cudaMemset(d->status.p, 0, 64));
+  *out = d.release();
+  return GF2C_OK;
+}
+
+int gf2c_decoder_create(const gf2c_code* code, const gf2c_decoder_opts* opts, gf2c_decoder** out) {
+  const gf2c_code* codes[1] = {code};
+  return gf2c_decoder_create_multi(codes, 1, opts, out);
+}
+
+int gf2c_decoder_destroy(gf2c_decoder* dec) {
+  delete dec;
+  return GF2C_OK;
+}
+
+int gf2c_decoder_last_launches(const gf2c_decoder* dec, int32_t* launches) {
+  if (!dec || !launches) return set_error(GF2C_ERR_INVALID_ARG, "NULL argument");
+  *launches = dec->last_launches;
+  return GF2C_OK;
+}
+
+static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaStream_t st) {
+  a.codes = (const DevCode*)d->d_codes.p;
+  a.ncodes = (int)d->codes.size();
+  a.frames = frames;
+  a.queue = (unsigned long long*)d->queue.p;
+  a.work = (char*)d->work.p;
+  a.work_stride = d->work_stride;
+  a.app_offset = d->app_offset;
+  a.smem_app_floats = d->smem_app_floats;
+  a.bitmap_words = d->bitmap_words;
+  a.alpha = (const float*)d->alpha.p;
+  a.beta = (const float*)d->beta.p;
+  a.nms_iters = d->opts.algorithm == GF2C_ALGO_NMS ? d->nms_iters : 0;
+  a.nms_L = d->nms_L;
+  a.early_stop = d->opts.early_stop;
+  a.status = (int*)d->status.p;
+  GF2C_CUDA(cudaMemsetAsync(d->queue.p, 0, sizeof(unsigned long long), st));
+  int grid = (int)std::min<int64_t>(d->grid, frames);
+  d->last_launches = 1;
+  return launch_decode(d->opts.algorithm, d->opts.msg_dtype, d->opts.schedule, d->dcmax, a, grid,
+                       d->threads, d->smem, st);
+}
+
+static int check_status(gf2c_decoder* d, cudaStream_t st) {
+  int h = 0;
+  GF2C_CUDA(cudaMemcpyAsync(&h, d->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  GF2C_CUDA(cudaStreamSynchronize(st));
+  if (h) {
+    cudaMemsetAsync(d->status.p, 0, sizeof(int), st);
+    return set_error(GF2C_ERR_INVALID_ARG, "a frame referenced a code id outside the decoder's codes");
+  }
+  return GF2C_OK;
+}
+
+int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32_t max_iter, uint64_t* msg_bits,
+                      int32_t* iterations, uint8_t* converged, uint8_t* syndrome_ok, float* beliefs, int32_t mem,
+                      void* stream) {
+  if (!dec || frames < 0 || max_iter < 0 || (frames > 0 && !llr))
+    return set_error(GF2C_ERR_INVALID_ARG, "bad arguments");
+  int rc = check_mem(mem);
+  if (rc || frames == 0) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const HostCode& h = *dec->codes[0]->h;
+  DecodeArgs a{};
+  a.max_iter = max_iter;
+  if (mem == GF2C_MEM_DEVICE) {
+    a.llr = llr;
+    a.msg = msg_bits;
+    a.iters = iterations;
+    a.conv = converged;
+    a.synd_ok = syndrome_ok;
+    a.beliefs = beliefs;
+    return launch_decoder(dec, a, frames, st);
+  }
+  const int wk = (int)((h.k + 63) / 64);
+  size_t bl = (size_t)frames * h.n * 4, bm = (size_t)frames * wk * 8;
+  if ((rc = dec->s_llr.ensure(bl)) || (rc = dec->s_msg.ensure(bm)) || (rc = dec->s_it.ensure(frames * 4)) ||
+      (rc = dec->s_cv.ensure(frames)) || (rc = dec->s_so.ensure(frames)))
+    return rc;
+  if (beliefs && (rc = dec->s_bel.ensure(bl))) return rc;
+  GF2C_CUDA(cudaMemcpyAsync(dec->s_llr.p, llr, bl, cudaMemcpyHostToDevice, st));
+  a.llr = (const float*)dec->s_llr.p;
+  a.msg = msg_bits ? (uint64_t*)dec->s_msg.p : nullptr;
+  a.iters = (int32_t*)dec->s_it.p;
+  a.conv = (uint8_t*)dec->s_cv.p;
+  a.synd_ok = (uint8_t*)dec->s_so.p;
+  a.beliefs = beliefs ? (float*)dec->s_bel.p : nullptr;
+  if ((rc = launch_decoder(dec, a, frames, st))) return rc;
+  if (msg_bits) GF2C_CUDA(cudaMemcpyAsync(msg_bits, dec->s_msg.p, bm, cudaMemcpyDeviceToHost, st));
+  if (iterations) GF2C_CUDA(cudaMemcpyAsync(iterations, dec->s_it.p, frames * 4, cudaMemcpyDeviceToHost, st));
+  if (converged) GF2C_CUDA(cudaMemcpyAsync(converged, dec->s_cv.p, frames, cudaMemcpyDeviceToHost, st));
+  if (syndrome_ok) GF2C_CUDA(cudaMemcpyAsync(syndrome_ok, dec->s_so.p, frames, cudaMemcpyDeviceToHost, st));
+  if (beliefs) GF2C_CUDA(cudaMemcpyAsync(beliefs, dec->s_bel.p, bl, cudaMemcpyDeviceToHost, st));
+  return check_status(dec, st);
+}
+
+int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_offset, const int32_t* code_id,
+                      const int32_t* max_iter, int64_t frames, uint64_t* msg_bits, const int64_t* msg_offset,
+                      int32_t* iterations, uint8_t* converged, uint8_t* syndrome_ok, int32_t use_graph,
+                      int32_t mem, void* stream) {
+  if (!dec || frames < 0 || (frames > 0 && (!llr || !llr_offset || !code_id || !max_iter)))
+    return set_error(GF2C_ERR_INVALID_ARG, "bad arguments");
+  if (msg_bits && !msg_offset) return set_error(GF2C_ERR_INVALID_ARG, "msg_bits needs msg_offset");
+  int rc = check_mem(mem);
+  if (rc || frames == 0) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  DecodeArgs a{};
+  if (mem == GF2C_MEM_DEVICE) {
+    a.llr = llr;
+    a.llr_off = llr_offset;
+    a.code_id = code_id;
+    a.max_iter_arr = max_iter;
+    a.msg = msg_bits;
+    a.msg_off = msg_offset;
+    a.iters = iterations;
+    a.conv = converged;
+    a.synd_ok = syndrome_ok;
+    if (!use_graph) return launch_decoder(dec, a, frames, st);
+    GraphKey key;
+    key.v = {(uintptr_t)llr, (uintptr_t)llr_offset, (uintptr_t)code_id, (uintptr_t)max_iter,
+             (uintptr_t)msg_bits, (uintptr_t)msg_offset, (uintptr_t)iterations, (uintptr_t)converged,
+             (uintptr_t)syndrome_ok, (uintptr_t)frames};
+    // Graphs are captured and replayed on the decoder's own stream, ordered
+    // after / before the caller's stream with events (the legacy default
+    // stream cannot be captured).
+    if (!dec->gstream) {
+      GF2C_CUDA(cudaStreamCreateWithFlags(&dec->gstream, cudaStreamNonBlocking));
+      GF2C_CUDA(cudaEventCreateWithFlags(&dec->ev_in, cudaEventDisableTiming));
+      GF2C_CUDA(cudaEventCreateWithFlags(&dec->ev_out, cudaEventDisableTiming));
+    }
+    cudaStream_t gs = dec->gstream;
+    auto it = dec->graphs.find(key);
+    if (it == dec->graphs.end()) {
+      cudaGraph_t g;
+      GF2C_CUDA(cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal));
+      rc = launch_decoder(dec, a, frames, gs);
+      cudaError_t e = cudaStreamEndCapture(gs, &g);
+      if (rc) return rc;
+      if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");
+      cudaGraphExec_t ex;
+      e = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return cuda_error(e, "cudaGraphInstantiate");
+      it = dec->graphs.emplace(key, ex).first;
+    }
+    GF2C_CUDA(cudaEventRecord(dec->ev_in, st));
+    GF2C_CUDA(cudaStreamWaitEvent(gs, dec->ev_in, 0));
+    GF2C_CUDA(cudaGraphLaunch(it->second, gs));
+    GF2C_CUDA(cudaEventRecord(dec->ev_out, gs));
+    GF2C_CUDA(cudaStreamWaitEvent(st, dec->ev_out, 0));
+    dec->last_launches = 1;
+    return GF2C_OK;
+  }
+  // host memory: validate ids and offsets, stage everything
+  int64_t llr_total = 0, msg_total = 0;
+  for (int64_t f = 0; f < frames; f++) {
+    int c = code_id[f];
+    if (c < 0 || c >= (int)dec->codes.size()) return set_error(GF2C_ERR_INVALID_ARG, "code_id out of range");
+    if (max_iter[f] < 0 || llr_offset[f] < 0 || (msg_bits && msg_offset[f] < 0))
+      return set_error(GF2C_ERR_INVALID_ARG, "negative offset or max_iter");
+    const HostCode& h = *dec->codes[c]->h;
+    llr_total = std::max<int64_t>(llr_total, llr_offset[f] + h.n);
+    if (msg_bits) msg_total = std::max<int64_t>(msg_total, msg_offset[f] + (h.k + 63) / 64);
+  }
+  if ((rc = dec->s_llr.ensure(llr_total * 4)) || (rc = dec->s_msg.ensure(std::max<int64_t>(msg_total, 1) * 8)) ||
+      (rc = dec->s_it.ensure(frames * 4)) || (rc = dec->s_cv.ensure(frames)) || (rc = dec->s_so.ensure(frames)) ||
+      (rc = dec->s_off1.ensure(frames * 8)) || (rc = dec->s_off2.ensure(frames * 8)) ||
+      (rc = dec->s_cid.ensure(frames * 4)) || (rc = dec->s_mit.ensure(frames * 4)))
+    return rc;
+  GF2C_CUDA(cudaMemcpyAsync(dec->s_llr.p, llr, llr_total * 4, cudaMemcpyHostToDevice, st));
+  GF2C_CUDA(cudaMemcpyAsync(dec->s_off1.p, llr_offset, frames * 8, cudaMemcpyHostToDevice, st));
+  if (msg_bits) GF2C_CUDA(cudaMemcpyAsync(dec->s_off2.p, msg_offset, frames * 8, cudaMemcpyHostToDevice, st));
+  GF2C_CUDA(cudaMemcpyAsync(dec->s_cid.p, code_id, frames * 4, cudaMemcpyHostToDevice, st));
+  GF2C_CUDA(cudaMemcpyAsync(dec->s_mit.p, max_iter, frames * 4, cudaMemcpyHostToDevice, st));
+  a.llr = (const float*)dec->s_llr.p;
+  a.llr_off = (const int64_t*)dec->s_off1.p;
+  a.code_id = (const int32_t*)dec->s_cid.p;
+  a.max_iter_arr = (const int32_t*)dec->s_mit.p;
+  a.msg = msg_bits ? (uint64_t*)dec->s_msg.p : nullptr;
+  a.msg_off = msg_bits ? (const int64_t*)dec->s_off2.p : nullptr;
+  a.iters = (int32_t*)dec->s_it.p;
+  a.conv = (uint8_t*)dec->s_cv.p;
+  a.synd_ok = (uint8_t*)dec->s_so.p;
+  if ((rc = launch_decoder(dec, a, frames, st))) return rc;
+  if (msg_bits) GF2C_CUDA(cudaMemcpyAsync(msg_bits, dec->s_msg.p, msg_total * 8, cudaMemcpyDeviceToHost, st));
+  if (iterations) GF2C_CUDA(cudaMemcpyAsync(iterations, dec->s_it.p, frames * 4, cudaMemcpyDeviceToHost, st));
+  if (converged) GF2C_CUDA(cudaMemcpyAsync(converged, dec->s_cv.p, frames, cudaMemcpyDeviceToHost, st));
+  if (syndrome_ok) GF2C_CUDA(cudaMemcpyAsync(syndrome_ok, dec->s_so.p, frames, cudaMemcpyDeviceToHost, st));
+  return check_status(dec, st);
+}
+
+}  // extern "C"

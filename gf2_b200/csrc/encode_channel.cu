@@ -1,0 +1,307 @@
+// gf2cuda encoder, syndrome and AWGN channel kernels (sm_100a).
+//
+// Encoder: the reference encodes with a dense k x m generator block
+// (RuEncodingMatrices::encode, crates/gf2-coding/src/ldpc/encoding/richardson_urbanke.rs:263-289,
+// 97.5% of its encode time in BitMatrix::matvec_transpose).  For DVB-T2 codes the
+// parity part of H is the staircase, so the same unique codeword is
+//   s = H_info u (one XOR per info edge),  p[i] = s[0] ^ ... ^ s[i]
+// i.e. an XOR-gather followed by a prefix-XOR scan, done here with warp ballots
+// and a block scan over 32-bit words.  Other codes use the dense generator
+// block of the right-to-left pivot search (the reference's columns).
+//
+// Syndrome: LdpcCode::syndrome (crates/gf2-coding/src/ldpc/core.rs:129-133).
+// Channel: BpskModulator / AwgnChannel (crates/gf2-coding/src/channel.rs:51-218) with
+// Philox4x32-10 and Box-Muller in place of rand_distr::Normal.
+#include "internal.h"
+#include "numeric.cuh"
+
+namespace gf2c {
+
+static constexpr int kEncThreads = 1024;
+
+// Bit i of a u32-word bit array.
+__device__ __forceinline__ uint32_t getbit(const uint32_t* w, int i) { return (w[i >> 5] >> (i & 31)) & 1u; }
+
+// Block-wide exclusive XOR scan of one bit per thread slot (count <= blockDim.x).
+__device__ __forceinline__ uint32_t block_xor_scan_excl(uint32_t bit, uint32_t* warp_tot) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+  const uint32_t below = __popc(bal & ((1u << lane) - 1u)) & 1u;
+  if (lane == 0) warp_tot[wid] = __popc(bal) & 1u;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    const uint32_t t = lane < nw ? warp_tot[lane] : 0u;
+    const uint32_t b2 = __ballot_sync(0xffffffffu, t);
+    const uint32_t ex = __popc(b2 & ((1u << lane) - 1u)) & 1u;
+    __syncwarp();
+    if (lane < nw) warp_tot[lane] = ex;
+  }
+  __syncthreads();
+  const uint32_t r = below ^ warp_tot[wid];
+  __syncthreads();
+  return r;
+}
+
+// Encodes the message bits u (k bits, u32 words in shared memory) into the
+// codeword cw (n bits, u32 words in shared memory).  scratch: >= words32(m) + 64 words.
+__device__ void encode_frame(const DevCode& C, const uint32_t* u, uint32_t* cw, uint32_t* scratch) {
+  const int n = C.n, k = C.k, m = C.m;
+  const int wn = (n + 31) >> 5, wk = (k + 31) >> 5, wm = (m + 31) >> 5;
+  uint32_t* par = scratch;          // m parity bits
+  uint32_t* warp_tot = scratch + wm;
+  if (C.enc_kind == 0) {
+    // s_p = XOR of the info bits of check p (natural check order)
+    for (int base = 0; base < m; base += blockDim.x) {
+      const int p = base + threadIdx.x;
+      uint32_t s = 0;
+      if (p < m) {
+        const int e1 = __ldg(&C.csr_ptr[p + 1]);
+        for (int e = __ldg(&C.csr_ptr[p]); e < e1; e++) {
+          const int v = __ldg(&C.csr_idx[e]);
+          if (v < k) s ^= getbit(u, v);
+        }
+      }
+      const uint32_t b = __ballot_sync(0xffffffffu, s);
+      if ((threadIdx.x & 31) == 0 && p < m) par[p >> 5] = b;
+    }
+    __syncthreads();
+    // prefix XOR over the m bits: in-word scan, then carry across words
+    for (int base = 0; base < wm; base += blockDim.x) {
+      const int w = base + threadIdx.x;
+      uint32_t x = w < wm ? par[w] : 0u;
+      x ^= x << 1;
+      x ^= x << 2;
+      x ^= x << 4;
+      x ^= x << 8;
+      x ^= x << 16;
+      const uint32_t carry_in = base > 0 ? (par[base - 1] >> 31) & 1u : 0u;
+      __syncthreads();
+      const uint32_t ex = block_xor_scan_excl(x >> 31, warp_tot) ^ carry_in;
+      if (w < wm) par[w] = ex ? ~x : x;
+      __syncthreads();
+    }
+    if (m & 31) {
+      if (threadIdx.x == 0) par[wm - 1] &= (1u << (m & 31)) - 1u;
+    }
+    __syncthreads();
+    // cw = [u | par]
+    for (int w = threadIdx.x; w < wn; w += blockDim.x) {
+      uint32_t out = 0;
+      const int lo = 32 * w;
+      if (lo + 32 <= k) {
+        out = u[w];
+      } else {
+        if (lo < k) out = u[w] & ((1u << (k - lo)) - 1u);
+        // parity bits p at codeword positions k + p
+        const int pstart = lo < k ? 0 : lo - k;     // first parity index in this word
+        const int bitpos = lo < k ? k - lo : 0;     // its bit position in this word
+        const int pw = pstart >> 5, ps = pstart & 31;
+        uint64_t two = (uint64_t)par[pw] | ((pw + 1 < wm) ? ((uint64_t)par[pw + 1] << 32) : 0ull);
+        uint32_t bits = (uint32_t)(two >> ps);
+        if (bitpos < 32) out |= bits << bitpos;
+        const int valid = n - lo;
+        if (valid < 32) out &= (1u << valid) - 1u;
+      }
+      cw[w] = out;
+    }
+    __syncthreads();
+  } else {
+    // parity word j (64 bits) = XOR over message bits i of P[i][j]
+    const int Wm = C.words_m;
+    uint64_t* par64 = (uint64_t*)scratch;  // Wm words (scratch sized for it)
+    for (int j = threadIdx.x; j < Wm; j += blockDim.x) {
+      uint64_t acc = 0;
+      for (int i = 0; i < k; i++)
+        if (getbit(u, i)) acc ^= __ldg(&C.enc_p[(size_t)i * Wm + j]);
+      par64[j] = acc;
+    }
+    for (int w = threadIdx.x; w < wn; w += blockDim.x) cw[w] = 0u;
+    __syncthreads();
+    for (int i = threadIdx.x; i < k; i += blockDim.x)
+      if (getbit(u, i)) {
+        const int c = __ldg(&C.enc_msg_cols[i]);
+        atomicOr(&cw[c >> 5], 1u << (c & 31));
+      }
+    for (int j = threadIdx.x; j < m; j += blockDim.x)
+      if ((par64[j >> 6] >> (j & 63)) & 1ull) {
+        const int c = __ldg(&C.enc_par_cols[j]);
+        atomicOr(&cw[c >> 5], 1u << (c & 31));
+      }
+    __syncthreads();
+  }
+  (void)wk;
+}
+
+// shared memory: u (wk32) + cw (wn32) + scratch (max(wm32 + 64, 2*Wm))
+static size_t encode_smem(const DevCode& C) {
+  const int wn = (C.n + 31) / 32, wk = (C.k + 31) / 32, wm = (C.m + 31) / 32;
+  const int scratch = std::max(wm + 64, 2 * C.words_m);
+  return (size_t)(wk + wn + scratch + 4) * 4;
+}
+
+__global__ void __launch_bounds__(kEncThreads) encode_kernel(const DevCode* __restrict__ Cp,
+                                                             const uint64_t* __restrict__ msg,
+                                                             long long frames, uint64_t* __restrict__ cw) {
+  extern __shared__ uint32_t sm[];
+  const DevCode C = *Cp;
+  const int wn = (C.n + 31) / 32, wk = (C.k + 31) / 32;
+  uint32_t* u = sm;
+  uint32_t* c = sm + wk;
+  uint32_t* scratch = c + wn;
+  for (long long f = blockIdx.x; f < frames; f += gridDim.x) {
+    const uint32_t* mi = (const uint32_t*)(msg + f * (long long)C.words_k);
+    for (int w = threadIdx.x; w < wk; w += blockDim.x) {
+      uint32_t x = mi[w];
+      const int rem = C.k - 32 * w;
+      if (rem < 32) x &= (1u << rem) - 1u;
+      u[w] = x;
+    }
+    __syncthreads();
+    encode_frame(C, u, c, scratch);
+    uint32_t* co = (uint32_t*)(cw + f * (long long)C.words_n);
+    for (int w = threadIdx.x; w < 2 * C.words_n; w += blockDim.x) co[w] = w < wn ? c[w] : 0u;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) syndrome_kernel(const DevCode* __restrict__ Cp,
+                                                       const uint64_t* __restrict__ cw, long long frames,
+                                                       uint64_t* __restrict__ synd, int32_t* __restrict__ weight) {
+  extern __shared__ uint32_t sm[];
+  __shared__ int s_w;
+  const DevCode C = *Cp;
+  const int wn = (C.n + 31) / 32;
+  for (long long f = blockIdx.x; f < frames; f += gridDim.x) {
+    const uint32_t* ci = (const uint32_t*)(cw + f * (long long)C.words_n);
+    for (int w = threadIdx.x; w < wn; w += blockDim.x) sm[w] = ci[w];
+    if (threadIdx.x == 0) s_w = 0;
+    __syncthreads();
+    uint32_t* so = synd ? (uint32_t*)(synd + f * (long long)C.words_m) : nullptr;
+    int cnt = 0;
+    for (int base = 0; base < 32 * 2 * C.words_m; base += blockDim.x) {
+      const int p = base + threadIdx.x;
+      uint32_t s = 0;
+      if (p < C.m) {
+        const int e1 = __ldg(&C.csr_ptr[p + 1]);
+        for (int e = __ldg(&C.csr_ptr[p]); e < e1; e++) s ^= getbit(sm, __ldg(&C.csr_idx[e]));
+      }
+      cnt += s;
+      const uint32_t b = __ballot_sync(0xffffffffu, s);
+      if ((threadIdx.x & 31) == 0 && so) so[p >> 5] = b;
+    }
+    atomicAdd(&s_w, cnt);
+    __syncthreads();
+    if (threadIdx.x == 0 && weight) weight[f] = s_w;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kEncThreads) channel_kernel(const DevCode* __restrict__ Cp, uint2 key,
+                                                              unsigned long long frame0, long long frames,
+                                                              const double* __restrict__ sigma2,
+                                                              uint64_t* __restrict__ info,
+                                                              uint64_t* __restrict__ cwo, float* __restrict__ llr) {
+  extern __shared__ uint32_t sm[];
+  const DevCode C = *Cp;
+  const int wn = (C.n + 31) / 32, wk = (C.k + 31) / 32;
+  uint32_t* u = sm;
+  uint32_t* c = sm + wk;
+  uint32_t* scratch = c + wn;
+  for (long long f = blockIdx.x; f < frames; f += gridDim.x) {
+    const uint32_t fr = (uint32_t)(frame0 + (unsigned long long)f);
+    // info bits: 128 per Philox call, counter (block, frame, 1, 0)
+    for (int blk = threadIdx.x; blk * 128 < C.k; blk += blockDim.x) {
+      const uint4 r = philox4x32_10(make_uint4((uint32_t)blk, fr, 1u, 0u), key);
+      const uint32_t wv[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int w = blk * 4 + q;
+        if (w < wk) {
+          uint32_t x = wv[q];
+          const int rem = C.k - 32 * w;
+          if (rem < 32) x &= (1u << rem) - 1u;
+          u[w] = x;
+        }
+      }
+    }
+    __syncthreads();
+    encode_frame(C, u, c, scratch);
+    if (info) {
+      uint32_t* io = (uint32_t*)(info + f * (long long)C.words_k);
+      for (int w = threadIdx.x; w < 2 * C.words_k; w += blockDim.x) io[w] = w < wk ? u[w] : 0u;
+    }
+    if (cwo) {
+      uint32_t* co = (uint32_t*)(cwo + f * (long long)C.words_n);
+      for (int w = threadIdx.x; w < 2 * C.words_n; w += blockDim.x) co[w] = w < wn ? c[w] : 0u;
+    }
+    if (llr) {
+      const double s2 = sigma2[f];
+      const double sigma = __dsqrt_rn(s2);
+      float* lo = llr + f * (long long)C.n;
+      for (int pair = threadIdx.x; 2 * pair < C.n; pair += blockDim.x) {
+        const uint4 r = philox4x32_10(make_uint4((uint32_t)pair, fr, 2u, 0u), key);
+        const unsigned long long a = (((unsigned long long)r.x << 32) | r.y) >> 11;
+        const unsigned long long b = (((unsigned long long)r.z << 32) | r.w) >> 11;
+        const double u1 = __dmul_rn((double)(a + 1ull), 1.1102230246251565404e-16);
+        const double u2 = __dmul_rn((double)b, 1.1102230246251565404e-16);
+        const double rad = __dsqrt_rn(__dmul_rn(-2.0, log_d(u1)));
+        double sn, cs;
+        sincos_2pi_d(u2, &sn, &cs);
+        const double z[2] = {__dmul_rn(rad, cs), __dmul_rn(rad, sn)};
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int i = 2 * pair + h;
+          if (i < C.n) {
+            const double sym = getbit(c, i) ? -1.0 : 1.0;
+            const double y = __dadd_rn(sym, __dmul_rn(sigma, z[h]));
+            lo[i] = __double2float_rn(__ddiv_rn(__dmul_rn(2.0, y), s2));
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+static int grid_for(long long frames) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long g = std::min<long long>(frames, (long long)sms * 2);
+  return (int)std::max<long long>(g, 1);
+}
+
+int launch_encode(const DevCode* dcode, const DevCode& h, const uint64_t* msg, long long frames,
+                  uint64_t* cw, cudaStream_t st) {
+  if (frames <= 0) return GF2C_OK;
+  size_t smem = encode_smem(h);
+  GF2C_CUDA(cudaFuncSetAttribute(encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  encode_kernel<<<grid_for(frames), kEncThreads, smem, st>>>(dcode, msg, frames, cw);
+  GF2C_CUDA(cudaGetLastError());
+  return GF2C_OK;
+}
+
+int launch_syndrome(const DevCode* dcode, const DevCode& h, const uint64_t* cw, long long frames,
+                    uint64_t* synd, int32_t* weight, cudaStream_t st) {
+  if (frames <= 0) return GF2C_OK;
+  size_t smem = (size_t)((h.n + 31) / 32) * 4;
+  GF2C_CUDA(cudaFuncSetAttribute(syndrome_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  syndrome_kernel<<<grid_for(frames), 256, smem, st>>>(dcode, cw, frames, synd, weight);
+  GF2C_CUDA(cudaGetLastError());
+  return GF2C_OK;
+}
+
+int launch_channel(const DevCode* dcode, const DevCode& h, uint64_t seed, uint64_t frame0,
+                   long long frames, const double* sigma2, uint64_t* info, uint64_t* cw, float* llr,
+                   cudaStream_t st) {
+  if (frames <= 0) return GF2C_OK;
+  size_t smem = encode_smem(h);
+  GF2C_CUDA(cudaFuncSetAttribute(channel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+  channel_kernel<<<grid_for(frames), kEncThreads, smem, st>>>(dcode, key, frame0, frames, sigma2, info, cw, llr);
+  GF2C_CUDA(cudaGetLastError());
+  return GF2C_OK;
+}
+
+}  // namespace gf2c

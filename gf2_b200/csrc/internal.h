@@ -1,0 +1,165 @@
+// gf2cuda internal declarations: host code graph, device layout, kernel args.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gf2cuda.h"
+
+namespace gf2c {
+
+// ---------------------------------------------------------------------------
+// Device-side description of one code ("check groups" x "slots").
+//
+// Check nodes are grouped into check groups (CG).  For QC / DVB-T2 codes a CG
+// is one row group of Z checks (the layer of the layered schedule); for other
+// codes a CG is a run of up to 256 consecutive checks.  Inside a CG every check
+// has the same number of slots dc (shorter rows are padded with var = -1), and
+// the c2v message of slot i of check t lives at edge slot edge0 + i*nchk + t,
+// so a warp of consecutive checks touches consecutive message addresses.
+//
+// Variable nodes are grouped into var groups (VG) of vgs consecutive variables;
+// vg_slot lists, for slot i of variable j, the edge slot of its i-th edge in
+// ascending ORIGINAL check order (the reference's summation order), -1 = pad.
+// ---------------------------------------------------------------------------
+struct DevCode {
+  int n, m, k;
+  int ncg, nvg, vgs;
+  int e_slots;
+  int max_dc, max_dv;
+  int words_k, words_n, words_m;   // ceil(x/64)
+  int layered_ok;                  // CGs are layers usable by the layered schedule
+  int max_nchk;                    // largest CG
+  const int4* cg;                  // {chk_begin, nchk, dc, edge0}
+  const uint32_t* cg_sync;         // layered: bit i = barrier after slot i (dup variables)
+  const int* slot_var;             // [e_slots]
+  const uint16_t* chk_cg;          // [m] flattened check -> CG
+  const int2* vg;                  // {dv, vedge0}
+  const int* vg_slot;              // VG-major, [vg][i][j]
+  const int* csr_ptr;              // natural order H (m + 1)
+  const int* csr_idx;              // (nnz)
+  // encoder
+  int enc_kind;                    // 0 = DVB-T2 accumulator, 1 = dense generator
+  const uint64_t* enc_p;           // kind 1: k rows of words_m words (parity j of row i)
+  const int* enc_msg_cols;         // kind 1: k message columns
+  const int* enc_par_cols;         // kind 1: m parity columns
+};
+
+// Host-side code (reference-exact sparse structure + device layout plan).
+struct HostCode {
+  int64_t n = 0, m = 0, k = 0;
+  std::vector<int64_t> row_ptr, row_idx;   // CSR, columns ascending (sparse.rs:166-203)
+  std::vector<int64_t> col_ptr, col_idx;   // CSC, rows ascending (sparse.rs:297-328)
+  std::vector<int64_t> col_edge;           // CSC slot -> CSR edge
+  int kind = 0;                            // 0 edges, 1 QC, 2 DVB-T2
+  int z = 0, q = 0;
+  int dvb_index = -1;
+  std::vector<int32_t> qc_base;            // QC: mb x nb
+  int mb = 0, nb = 0;
+
+  // layout plan
+  std::vector<int4> cg;
+  std::vector<uint32_t> cg_sync;
+  std::vector<int> slot_var;
+  std::vector<uint16_t> chk_cg;
+  std::vector<int2> vg;
+  std::vector<int> vg_slot;
+  int vgs = 0, max_dc = 0, max_dv = 0, e_slots = 0, layered_ok = 0, max_nchk = 0;
+  std::vector<int64_t> cg_checks;          // original check of each flattened check
+
+  // encoder (generic)
+  int enc_kind = 0;
+  bool enc_ready = false;
+  int enc_status = GF2C_OK;
+  std::vector<uint64_t> enc_p;
+  std::vector<int> enc_msg_cols, enc_par_cols;
+
+  // device copy (lazily uploaded per device)
+  std::mutex dev_mu;
+  int dev_id = -1;
+  DevCode dev{};
+  std::vector<void*> dev_allocs;
+  ~HostCode();
+};
+
+struct KernelShape {
+  int threads = 0;
+  int blocks_per_sm = 0;
+};
+
+}  // namespace gf2c
+
+struct gf2c_code {
+  std::unique_ptr<gf2c::HostCode> h;
+};
+
+namespace gf2c {
+
+// error helpers
+int set_error(int code, const std::string& msg);
+int cuda_error(cudaError_t e, const char* what);
+#define GF2C_CUDA(call)                                        \
+  do {                                                          \
+    cudaError_t _e = (call);                                    \
+    if (_e != cudaSuccess) return ::gf2c::cuda_error(_e, #call); \
+  } while (0)
+
+// host code construction (code_host.cpp)
+int build_dvbt2(int frame, int rate, HostCode& c);
+int build_qc(const int32_t* base, int mb, int nb, int z, HostCode& c);
+int build_edges(int64_t m, int64_t n, const int64_t* pairs, int64_t count, HostCode& c);
+int prepare_encoder(HostCode& c);
+int upload_code(HostCode& c);  // uploads the device layout on the current device
+
+// ---------------------------------------------------------------------------
+// Kernel arguments
+// ---------------------------------------------------------------------------
+struct DecodeArgs {
+  const DevCode* codes;            // device array of ncodes
+  int ncodes;
+  const float* llr;
+  const int64_t* llr_off;          // nullable: frame f at f * n
+  const int32_t* code_id;          // nullable: code 0
+  const int32_t* max_iter_arr;     // nullable: max_iter for all
+  int max_iter;
+  uint64_t* msg;
+  const int64_t* msg_off;          // nullable: frame f at f * words_k
+  int32_t* iters;
+  uint8_t* conv;
+  uint8_t* synd_ok;
+  float* beliefs;                  // nullable
+  long long frames;
+  unsigned long long* queue;       // work counter, zero at launch
+  char* work;                      // per-CTA workspace
+  long long work_stride;           // bytes per CTA
+  long long app_offset;            // offset of the global APP inside a CTA workspace
+  int smem_app_floats;             // APP kept in shared memory when n <= this
+  int bitmap_words;                // 32-bit words of the hard-decision bitmap
+  const float* alpha;              // NMS weights [nms_iters][nms_L]
+  const float* beta;
+  int nms_iters;
+  int nms_L;
+  int early_stop;
+  int* status;                     // kernel-side error flag
+};
+
+int launch_decode(int algo, int msg16, int sched, int dcmax, const DecodeArgs& a, int grid,
+                  int threads, size_t smem, cudaStream_t st);
+int prepare_decode(int algo, int msg16, int sched, int dcmax, size_t smem, int threads,
+                   int* blocks_per_sm);
+int decode_dcmax_bucket(int max_dc);
+size_t decode_smem_bytes(int smem_app_floats, int bitmap_words);
+
+int launch_syndrome(const DevCode* dcode, const DevCode& hcode, const uint64_t* cw, long long frames,
+                    uint64_t* synd, int32_t* weight, cudaStream_t st);
+int launch_encode(const DevCode* dcode, const DevCode& hcode, const uint64_t* msg, long long frames,
+                  uint64_t* cw, cudaStream_t st);
+int launch_channel(const DevCode* dcode, const DevCode& hcode, uint64_t seed, uint64_t frame0,
+                   long long frames, const double* sigma2, uint64_t* info, uint64_t* cw, float* llr,
+                   cudaStream_t st);
+
+}  // namespace gf2c

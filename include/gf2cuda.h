@@ -1,0 +1,188 @@
+/* gf2cuda -- B200-native (sm_100a) batched LDPC encoder / decoder.
+ *
+ * C ABI of the library.  It replaces the belief-propagation path of the
+ * erankavija/gf2 `gf2-coding` crate (all paths below are relative to
+ * crates/gf2-coding/src/ of that project):
+ *
+ *   LdpcCode::{dvb_t2_normal, dvb_t2_short}     ldpc/core.rs:197-262
+ *   LdpcCode::from_quasi_cyclic                 ldpc/core.rs:168-173
+ *   LdpcCode::from_edges                        ldpc/core.rs:96-104
+ *   LdpcCode::{n, m, k, rate}                   ldpc/core.rs:107-124
+ *   LdpcCode::{syndrome, is_valid_codeword}     ldpc/core.rs:129-138
+ *   LdpcDecoder::new                            ldpc/core.rs:653-697
+ *   LdpcDecoder::decode_batch                   ldpc/core.rs:729-756
+ *   IterativeSoftDecoder::decode_iterative      traits.rs:335, ldpc/core.rs:889-938
+ *   LdpcEncoder::{encode, encode_batch}         ldpc/core.rs:1106-1132, traits.rs:206
+ *   AwgnChannel / BpskModulator                 channel.rs:51-218
+ *
+ * Conventions
+ *   - Every function returns an int status (GF2C_OK = 0); nothing aborts or
+ *     panics.  gf2c_last_error() gives a message for the calling thread.
+ *   - Bit vectors are packed in uint64_t words, bit i of a vector in word i/64
+ *     at bit position i%64 (the gf2-core BitVec layout), unused tail bits 0.
+ *     A batch of F vectors of length L occupies F * ceil(L/64) words.
+ *   - LLRs are IEEE f32, positive = bit 0 more likely (llr.rs:73-75).
+ *   - `mem` selects where the array arguments of one call live:
+ *     GF2C_MEM_HOST (pageable or pinned host memory; the library stages the
+ *     copies on `stream`) or GF2C_MEM_DEVICE (device pointers on the current
+ *     device).  `stream` is a cudaStream_t (NULL = legacy default stream).
+ *     Host-memory calls return after the results are in host memory;
+ *     device-memory calls are asynchronous on `stream`.
+ *   - Code handles are immutable after creation and may be shared by threads.
+ *     A decoder handle owns device workspace and must not be used by two
+ *     host threads at once.
+ */
+#ifndef GF2CUDA_H
+#define GF2CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define GF2C_OK 0
+#define GF2C_ERR_INVALID_ARG 1   /* bad pointer, size or enum value */
+#define GF2C_ERR_CUDA 2          /* a CUDA runtime call failed */
+#define GF2C_ERR_UNSUPPORTED 3   /* option not available for this code */
+#define GF2C_ERR_NOMEM 4         /* device or host allocation failed */
+#define GF2C_ERR_RANK 5          /* parity-check matrix is rank deficient */
+#define GF2C_ERR_KERNEL 6        /* a kernel reported an internal error */
+
+#define GF2C_MEM_HOST 0
+#define GF2C_MEM_DEVICE 1
+
+/* DvbParams::for_code (ldpc/dvb_t2/params.rs:56-85) */
+#define GF2C_DVBT2_NORMAL 0      /* n = 64800 */
+#define GF2C_DVBT2_SHORT 1       /* n = 16200 */
+#define GF2C_RATE_1_2 0
+#define GF2C_RATE_3_5 1
+#define GF2C_RATE_2_3 2
+#define GF2C_RATE_3_4 3
+#define GF2C_RATE_4_5 4
+#define GF2C_RATE_5_6 5
+
+/* Check-node rule of a decoder. */
+#define GF2C_ALGO_MINSUM 0  /* the reference's decoder: plain min-sum (core.rs:790-814),
+                               results bit-identical to LdpcDecoder up to the sign of zero */
+#define GF2C_ALGO_SPA 1     /* sum-product 2 atanh(prod tanh(x/2)) (core.rs:762-787,
+                               llr.rs:210-215), FP32, |extrinsic product| <= 1 - 2^-23 */
+#define GF2C_ALGO_NMS 2     /* normalised + offset min-sum (llr.rs:352-399) with one
+                               (alpha, beta) per iteration and row group */
+#define GF2C_SCHED_FLOODING 0  /* decode_iterative's schedule (core.rs:909-924) */
+#define GF2C_SCHED_LAYERED 1   /* row-group layered schedule (QC and DVB-T2 codes) */
+#define GF2C_MSG_F32 0
+#define GF2C_MSG_F16 1         /* messages stored as binary16, arithmetic in f32 */
+
+typedef struct gf2c_code gf2c_code;
+typedef struct gf2c_decoder gf2c_decoder;
+
+typedef struct {
+  int32_t algorithm;        /* GF2C_ALGO_* */
+  int32_t schedule;         /* GF2C_SCHED_* */
+  int32_t msg_dtype;        /* GF2C_MSG_* */
+  int32_t early_stop;       /* 1 = stop a frame when its syndrome is zero (the reference
+                               always does); 0 = run every frame for max_iter iterations */
+  const float* nms_alpha;   /* GF2C_ALGO_NMS: host array [nms_iters][layers] */
+  const float* nms_beta;    /* GF2C_ALGO_NMS: host array [nms_iters][layers] */
+  int32_t nms_iters;        /* rows of the weight arrays; iteration t uses row min(t, nms_iters-1) */
+  int32_t threads_per_block;/* 0 = library choice (autotuned when a tuning entry exists) */
+  int32_t blocks_per_sm;    /* 0 = library choice */
+} gf2c_decoder_opts;
+
+/* Fills opts with the reference behaviour: min-sum, flooding, f32, early stop. */
+void gf2c_decoder_opts_default(gf2c_decoder_opts* opts);
+
+const char* gf2c_last_error(void);
+const char* gf2c_version(void);
+
+/* ---- codes ---- */
+/* LdpcCode::dvb_t2_normal / dvb_t2_short (core.rs:197-262). */
+int gf2c_code_create_dvbt2(int32_t frame_size, int32_t rate, gf2c_code** out);
+/* LdpcCode::from_quasi_cyclic (core.rs:168-173, 578-605): base is mb x nb row-major,
+ * -1 = zero block, otherwise a right shift in [0, z). */
+int gf2c_code_create_qc(const int32_t* base, int32_t mb, int32_t nb, int32_t z, gf2c_code** out);
+/* LdpcCode::from_edges (core.rs:96-104): pairs = count (check, variable) pairs;
+ * repeated pairs cancel in pairs (GF(2) XOR, sparse.rs:166-203). */
+int gf2c_code_create_edges(int64_t m, int64_t n, const int64_t* pairs, int64_t count,
+                           gf2c_code** out);
+int gf2c_code_destroy(gf2c_code* code);
+/* n, m, k = max(n - m, 0), nonzeros of H, row groups usable by the layered schedule
+ * (0 when the code has none).  Any output pointer may be NULL. */
+int gf2c_code_dims(const gf2c_code* code, int64_t* n, int64_t* m, int64_t* k, int64_t* nnz,
+                   int32_t* layers);
+/* H as CSR in the reference's order (rows ascending, columns ascending): indptr
+ * has m+1 entries, indices nnz. */
+int gf2c_code_csr(const gf2c_code* code, int64_t* indptr, int64_t* indices);
+
+/* LdpcCode::syndrome over a batch (core.rs:129-133): synd = H cw, packed m bits per
+ * frame; weight (nullable) = popcount per frame (0 = valid codeword, core.rs:135-138). */
+int gf2c_syndrome_batch(const gf2c_code* code, const uint64_t* cw_bits, int64_t frames,
+                        uint64_t* synd_bits, int32_t* weight, int32_t mem, void* stream);
+
+/* ---- encoder ---- */
+/* LdpcEncoder::encode_batch (core.rs:1106-1132): systematic codewords.  The message
+ * bits occupy the non-pivot columns of a right-to-left RREF of H in ascending order
+ * and the parity bits the pivot columns (richardson_urbanke.rs:158-289); for DVB-T2
+ * codes that is [message | parity] with the staircase accumulator. */
+int gf2c_encode_batch(const gf2c_code* code, const uint64_t* msg_bits, int64_t frames,
+                      uint64_t* cw_bits, int32_t mem, void* stream);
+
+/* ---- channel ---- */
+/* Seeded synthetic frames: uniform info bits (Philox4x32-10, key = seed, counter
+ * = (block, frame0 + f, 1, 0)), systematic encoding, BPSK 0 -> +1 / 1 -> -1
+ * (channel.rs:51-57), AWGN with variance sigma2[f] (Box-Muller, counter
+ * (pair, frame0 + f, 2, 0)) and LLR = (f32)(2 y / sigma2[f]) (channel.rs:100-102).
+ * Any of info_bits / cw_bits / llr may be NULL.  sigma2 has `frames` entries, in
+ * the same memory space as the outputs. */
+int gf2c_channel_awgn(const gf2c_code* code, uint64_t seed, uint64_t frame0, int64_t frames,
+                      const double* sigma2, uint64_t* info_bits, uint64_t* cw_bits, float* llr,
+                      int32_t mem, void* stream);
+/* AwgnChannel::from_eb_n0_db (channel.rs:153-158): 1 / (2 rate 10^(ebn0/10)). */
+double gf2c_sigma2_from_ebn0(double ebn0_db, double rate);
+
+/* ---- decoder ---- */
+/* LdpcDecoder::new (core.rs:653-697).  One decoder may serve several codes (a mixed
+ * batch): gf2c_decoder_create_multi takes ncodes code handles, which must outlive it. */
+int gf2c_decoder_create(const gf2c_code* code, const gf2c_decoder_opts* opts,
+                        gf2c_decoder** out);
+int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes,
+                              const gf2c_decoder_opts* opts, gf2c_decoder** out);
+int gf2c_decoder_destroy(gf2c_decoder* dec);
+
+/* LdpcDecoder::decode_batch (core.rs:729-756) over `frames` frames of the decoder's
+ * (first) code, each decoded as IterativeSoftDecoder::decode_iterative (core.rs:889-938):
+ *   llr         frames x n f32, frame-major
+ *   max_iter    iteration budget (>= 0; 0 returns the all-zero word, like a fresh
+ *               reference decoder)
+ *   msg_bits    frames x ceil(k/64) words: hard decisions of the first k bits
+ *               (core.rs:930-935)                                   (nullable)
+ *   iterations  frames int32: DecoderResult::iterations            (nullable)
+ *   converged   frames uint8: DecoderResult::converged             (nullable)
+ *   syndrome_ok frames uint8: DecoderResult::syndrome_check_passed (nullable)
+ *   beliefs     frames x n f32 final posterior LLRs                (nullable)
+ * frames == 0 is a no-op. */
+int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32_t max_iter,
+                      uint64_t* msg_bits, int32_t* iterations, uint8_t* converged,
+                      uint8_t* syndrome_ok, float* beliefs, int32_t mem, void* stream);
+
+/* Mixed batch in one persistent launch: frame f uses code code_id[f] (index into the
+ * codes given at creation), reads n[code] LLRs at llr + llr_offset[f], writes
+ * ceil(k/64) words at msg_bits + msg_offset[f] (both in elements), and has its own
+ * budget max_iter[f].  Per-frame outputs as in gf2c_decode_batch.  With mem ==
+ * GF2C_MEM_DEVICE and use_graph = 1 the launch sequence is captured once per
+ * (frames, pointers) shape into a CUDA graph and replayed. */
+int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_offset,
+                      const int32_t* code_id, const int32_t* max_iter, int64_t frames,
+                      uint64_t* msg_bits, const int64_t* msg_offset, int32_t* iterations,
+                      uint8_t* converged, uint8_t* syndrome_ok, int32_t use_graph,
+                      int32_t mem, void* stream);
+
+/* Number of kernel launches issued by the last decode call of `dec`. */
+int gf2c_decoder_last_launches(const gf2c_decoder* dec, int32_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GF2CUDA_H */

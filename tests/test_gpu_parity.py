@@ -1,0 +1,266 @@
+"""GPU parity tests: the sm_100a library against the CPU oracle on the same
+seeded inputs, through the C ABI.
+
+Bars: reference min-sum decoding is bit-exact (hard decisions, iteration
+counts, flags, and posteriors, whose bits match the edge-indexed oracle and
+whose values equal the reference-faithful oracle's); encoder, syndrome and
+channel are bit-exact; the library's other decoders (sum-product FP32, layered,
+FP16 message storage, normalised/offset min-sum) are bit-exact against their
+oracle restatement.
+"""
+import numpy as np
+import pytest
+
+import gf2_b200 as g
+
+pytestmark = pytest.mark.gpu
+
+
+def dvb(idx):
+    return g.LdpcCode.dvb_t2_normal(idx) if idx < 6 else g.LdpcCode.dvb_t2_short(idx - 6)
+
+
+def unpack_msg(r, k):
+    return g.unpack_bits(r["msg"], k)
+
+
+def assert_same_decode(gpu, ora, k, bitwise=True):
+    assert (gpu["iters"] == ora["iters"]).all(), (gpu["iters"], ora["iters"])
+    assert (gpu["conv"] == ora["conv"]).all()
+    assert (gpu["synd_ok"] == ora["synd_ok"]).all()
+    assert (unpack_msg(gpu, k) == ora["msg"]).all()
+    if "beliefs" in gpu:
+        if bitwise:
+            assert (gpu["beliefs"].view(np.uint32) == ora["beliefs"].view(np.uint32)).all()
+        else:
+            assert (gpu["beliefs"] == ora["beliefs"]).all()
+
+
+def test_minsum_reference_parity_short_1_2(gpu, oracle):
+    """The BASELINE config-1 code and SNR: short 1/2, Eb/N0 1.0 dB, 50 iterations."""
+    code = g.LdpcCode.dvb_t2_short(g.CodeRate.Rate1_2)
+    ocode = oracle.Code.dvbt2(1, 0)
+    _, _, llr = ocode.channel(1, 0, 64, 1.0)
+    dec = g.LdpcDecoder(code)
+    r = dec.decode_arrays(llr, 50, beliefs=True)
+    assert_same_decode(r, ocode.decode(llr, 50), code.k(), bitwise=True)
+    assert_same_decode(r, ocode.decode_faithful(llr, 50), code.k(), bitwise=False)
+
+
+@pytest.mark.parametrize("idx,ebn0", [(1, 1.2), (5, 3.0), (9, 2.5)])
+def test_minsum_reference_parity_codes(gpu, oracle, idx, ebn0):
+    code = dvb(idx)
+    ocode = oracle.Code.dvbt2(idx // 6, idx % 6)
+    _, _, llr = ocode.channel(2, 0, 12, ebn0)
+    r = g.LdpcDecoder(code).decode_arrays(llr, 30, beliefs=True)
+    assert_same_decode(r, ocode.decode(llr, 30), code.k(), bitwise=True)
+    f = ocode.decode_faithful(llr[:4], 30)
+    assert (r["iters"][:4] == f["iters"]).all() and (r["beliefs"][:4] == f["beliefs"]).all()
+
+
+def test_decoder_kats(gpu):
+    # ldpc/core.rs:1149-1294 decoder tests, through the library
+    spc = g.LdpcCode.from_edges(1, 3, [(0, 0), (0, 1), (0, 2)])
+    dec = g.LdpcDecoder(spc)
+    r = dec.decode_iterative([g.Llr(10.0)] * 3, 10)
+    assert r.converged and r.syndrome_check_passed and r.decoded_bits.sum() == 0 and r.iterations <= 2
+    r = dec.decode_iterative([g.Llr(-5.0), g.Llr(-5.0), g.Llr(2.0)], 20)
+    assert r.converged and r.decoded_bits.sum() == 2
+    # no state leakage between decodes (core.rs:1188-1212)
+    for llr, ones in (([10, 10, 10], 0), ([-10, -10, 10], 2), ([10, 10, 10], 0)):
+        r = dec.decode_iterative(np.array(llr, np.float32), 10)
+        assert r.converged and r.decoded_bits.sum() == ones
+    res = g.LdpcDecoder.decode_batch(spc, [[10, 10, 10], [-10, -10, 10], [10, 10, 10]], 10)
+    assert [x.decoded_bits.sum() for x in res] == [0, 2, 0] and all(x.converged for x in res)
+    assert g.LdpcDecoder.decode_batch(spc, [], 10) == []
+    r = dec.decode_iterative(np.array([-10, -10, 10], np.float32), 0)
+    assert r.iterations == 0 and not r.converged and r.syndrome_check_passed and r.decoded_bits.sum() == 0
+    with pytest.raises(ValueError):
+        dec.decode_iterative([1.0, 2.0], 5)
+    short = g.LdpcCode.dvb_t2_short(g.CodeRate.Rate1_2)
+    d2 = g.LdpcDecoder(short)
+    r = d2.decode_iterative(np.full(short.n(), 5.0, np.float32), 10)   # ldpc_simd_validation.rs:27-43
+    assert r.converged
+    r = d2.decode_iterative(np.full(short.n(), np.inf, np.float32), 5)  # ldpc_validation.rs:349-422
+    assert r.converged and r.iterations == 1 and r.decoded_bits.sum() == 0
+
+
+@pytest.mark.parametrize("sched,msg16", [(0, False), (1, False), (1, True), (0, True)])
+def test_spa_parity(gpu, oracle, sched, msg16):
+    code = g.LdpcCode.dvb_t2_short(g.CodeRate.Rate1_2)
+    ocode = oracle.Code.dvbt2(1, 0)
+    _, _, llr = ocode.channel(3, 0, 24, 1.0)
+    dec = g.LdpcDecoder(code, algorithm=g.ALGO_SPA, schedule=sched, msg_dtype=g.MSG_F16 if msg16 else g.MSG_F32)
+    r = dec.decode_arrays(llr, 50, beliefs=True)
+    assert_same_decode(r, ocode.decode(llr, 50, algo=1, sched=sched, msg16=msg16), code.k())
+
+
+@pytest.mark.parametrize("idx", [1, 5, 0])
+def test_layered_dup_blocks_parity(gpu, oracle, idx):
+    """Normal 3/5 and 5/6 have up to 3 and 4 circulants in one (row group, block)."""
+    code = dvb(idx)
+    ocode = oracle.Code.dvbt2(idx // 6, idx % 6)
+    _, _, llr = ocode.channel(4, 0, 6, 1.6 if idx != 5 else 3.3)
+    for algo, oalgo in ((g.ALGO_MINSUM, 0), (g.ALGO_SPA, 1)):
+        dec = g.LdpcDecoder(code, algorithm=algo, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16)
+        r = dec.decode_arrays(llr, 20, beliefs=True)
+        assert_same_decode(r, ocode.decode(llr, 20, algo=oalgo, sched=1, msg16=True), code.k())
+
+
+@pytest.mark.parametrize("sched", [0, 1])
+def test_nms_parity(gpu, oracle, sched):
+    code = g.LdpcCode.dvb_t2_short(g.CodeRate.Rate3_5)
+    ocode = oracle.Code.dvbt2(1, 1)
+    _, _, llr = ocode.channel(6, 0, 16, 1.6)
+    rng = np.random.default_rng(0)
+    T, L = 6, code.layers()
+    a = (0.6 + 0.4 * rng.random((T, L))).astype(np.float32)
+    b = (0.3 * rng.random((T, L))).astype(np.float32)
+    dec = g.LdpcDecoder(code, algorithm=g.ALGO_NMS, schedule=sched, nms_alpha=a, nms_beta=b)
+    r = dec.decode_arrays(llr, 20, beliefs=True)
+    assert_same_decode(r, ocode.decode(llr, 20, algo=3, sched=sched, alpha=a, beta=b), code.k())
+
+
+def test_device_tensor_path_matches_host(gpu, oracle):
+    import torch
+    code = g.LdpcCode.dvb_t2_short(g.CodeRate.Rate2_3)
+    ocode = oracle.Code.dvbt2(1, 2)
+    _, _, llr = ocode.channel(8, 0, 40, 2.0)
+    dec = g.LdpcDecoder(code)
+    h = dec.decode_arrays(llr, 40)
+    d = dec.decode_tensors(torch.from_numpy(llr).to(gpu), 40)
+    torch.cuda.synchronize()
+    assert (d["msg"].cpu().numpy().view(np.uint64) == h["msg"]).all()
+    assert (d["iters"].cpu().numpy() == h["iters"]).all()
+    assert dec.last_launches() == 1
+
+
+@pytest.mark.parametrize("idx", range(12))
+def test_encoder_syndrome_parity(gpu, oracle, idx):
+    code = dvb(idx)
+    ocode = oracle.Code.dvbt2(idx // 6, idx % 6)
+    rng = np.random.default_rng(idx)
+    msg = rng.integers(0, 2, (5, code.k()), dtype=np.uint8)
+    msg[0] = 0
+    cw = g.LdpcEncoder(code).encode_packed(g.pack_bits(msg, code.k()))
+    assert (g.unpack_bits(cw, code.n()) == ocode.encode(msg)).all()
+    s, w = code.syndrome_batch(cw)
+    assert (w == 0).all() and (s == 0).all()
+    bad = g.unpack_bits(cw, code.n()).copy()
+    bad[1, 7] ^= 1
+    bad[2, code.n() - 1] ^= 1
+    s, w = code.syndrome_batch(g.pack_bits(bad, code.n()))
+    for f in range(5):
+        os_ = ocode.syndrome(bad[f])
+        assert w[f] == os_.sum()
+        assert (g.unpack_bits(s[f:f + 1], code.m())[0] == os_).all()
+
+
+def test_encoder_generic_codes(gpu, oracle):
+    spc = g.LdpcCode.from_edges(1, 3, [(0, 0), (0, 1), (0, 2)])
+    enc = g.LdpcEncoder(spc)
+    cws = enc.encode_batch([np.array(m, np.uint8) for m in ([0, 0], [1, 0], [0, 1], [1, 1])])
+    assert [c.tolist() for c in cws] == [[0, 0, 0], [1, 0, 1], [0, 1, 1], [1, 1, 0]]
+    assert enc.encode_batch([]) == []
+    base = [[0, 3, 1, -1, 2, 0], [2, -1, 4, 1, 0, 3], [-1, 1, 0, 3, 4, 1]]
+    q = g.LdpcCode.from_quasi_cyclic(g.QuasiCyclicLdpc(base, 7))
+    oq = oracle.Code.qc(base, 7)
+    msg = np.random.default_rng(5).integers(0, 2, (6, q.k()), dtype=np.uint8)
+    try:
+        ref = oq.encode(msg)
+    except oracle.OracleError:
+        pytest.skip("random QC base is rank deficient")
+    cw = g.LdpcEncoder(q).encode_packed(g.pack_bits(msg, q.k()))
+    assert (g.unpack_bits(cw, q.n()) == ref).all()
+
+
+@pytest.mark.parametrize("idx", [6, 1])
+def test_channel_parity(gpu, oracle, idx):
+    code = dvb(idx)
+    ocode = oracle.Code.dvbt2(idx // 6, idx % 6)
+    frames = 6
+    eb = np.array([0.5, 1.0, 1.5, 2.0, 2.5, 3.0])
+    s2 = np.array([oracle.sigma2(e, ocode.rate) for e in eb])
+    info, cw, llr = g.awgn_frames(code, 1234, 77, frames, s2)
+    oi, oc, ol = ocode.channel(1234, 77, frames, eb)
+    assert (g.unpack_bits(info, code.k()) == oi).all()
+    assert (g.unpack_bits(cw, code.n()) == oc).all()
+    assert (llr.view(np.uint32) == ol.view(np.uint32)).all()
+
+
+def test_mixed_batch_matches_single(gpu, oracle):
+    idxs = [6, 7, 11, 1]
+    codes = [dvb(i) for i in idxs]
+    dec = g.LdpcDecoder(codes[0], codes=codes)
+    rng = np.random.default_rng(2)
+    F = 20
+    cid = rng.integers(0, len(codes), F).astype(np.int32)
+    mit = rng.integers(0, 30, F).astype(np.int32)
+    llrs, lo, mo = [], [], []
+    off = moff = 0
+    for f in range(F):
+        oc = oracle.Code.dvbt2(idxs[cid[f]] // 6, idxs[cid[f]] % 6)
+        _, _, l = oc.channel(10, f, 1, 1.0 + 0.5 * rng.random() + (2.0 if idxs[cid[f]] == 11 else 0.0))
+        llrs.append(l[0])
+        lo.append(off)
+        mo.append(moff)
+        off += oc.n
+        moff += g.words(oc.k)
+    r = dec.decode_mixed_arrays(np.concatenate(llrs), lo, cid, mit, mo)
+    for f in range(F):
+        c = codes[cid[f]]
+        single = g.LdpcDecoder(c).decode_arrays(llrs[f][None, :], int(mit[f]))
+        assert r["iters"][f] == single["iters"][0]
+        assert r["conv"][f] == single["conv"][0]
+        w = g.words(c.k())
+        assert (r["msg"][mo[f]:mo[f] + w] == single["msg"][0]).all()
+
+
+def test_mixed_batch_graph_replay(gpu):
+    import torch
+    codes = [g.LdpcCode.dvb_t2_short(0), g.LdpcCode.dvb_t2_short(4)]
+    dec = g.LdpcDecoder(codes[0], codes=codes)
+    F = 16
+    cid = torch.tensor([f % 2 for f in range(F)], dtype=torch.int32, device=gpu)
+    n = [c.n() for c in codes]
+    lo = torch.tensor([sum(n[f % 2] for f in range(i)) for i in range(F)], dtype=torch.int64, device=gpu)
+    total = sum(n[f % 2] for f in range(F))
+    outs = []
+    for rep in range(3):
+        llr = torch.full((total,), 4.0, device=gpu)
+        mit = torch.full((F,), 10, dtype=torch.int32, device=gpu)
+        msg = torch.zeros(F * 256, dtype=torch.int64, device=gpu)
+        mo = torch.arange(F, dtype=torch.int64, device=gpu) * 256
+        it = torch.zeros(F, dtype=torch.int32, device=gpu)
+        cv = torch.zeros(F, dtype=torch.uint8, device=gpu)
+        so = torch.zeros(F, dtype=torch.uint8, device=gpu)
+        dec.decode_mixed_tensors(llr, lo, cid, mit, msg, mo, it, cv, so, use_graph=True)
+        torch.cuda.synchronize()
+        outs.append((it.cpu().numpy(), cv.cpu().numpy()))
+    for it, cv in outs:
+        assert (it == 1).all() and cv.all()
+
+
+def test_edge_cases(gpu, oracle):
+    # frames == 0 is a no-op; degree-1 check gives a zero message (core.rs:807-811)
+    code = g.LdpcCode.from_edges(3, 5, [(0, 0), (1, 1), (1, 2), (2, 2), (2, 3), (2, 4), (1, 4)])
+    ocode = oracle.Code.edges(3, 5, [(0, 0), (1, 1), (1, 2), (2, 2), (2, 3), (2, 4), (1, 4)])
+    dec = g.LdpcDecoder(code)
+    r = dec.decode_arrays(np.zeros((0, 5), np.float32), 5)
+    assert r["iters"].shape == (0,)
+    llr = np.random.default_rng(0).normal(1.0, 2.0, (50, 5)).astype(np.float32)
+    r = dec.decode_arrays(llr, 7, beliefs=True)
+    assert_same_decode(r, ocode.decode(llr, 7), code.k())
+    # high-degree generic code (dc up to 40 -> the 64-slot kernel)
+    rng = np.random.default_rng(1)
+    edges = [(r_, int(v)) for r_ in range(20) for v in rng.choice(200, size=int(rng.integers(2, 41)), replace=False)]
+    code = g.LdpcCode.from_edges(20, 200, edges)
+    ocode = oracle.Code.edges(20, 200, edges)
+    llr = rng.normal(2.0, 2.0, (30, 200)).astype(np.float32)
+    for algo, oalgo in ((g.ALGO_MINSUM, 0), (g.ALGO_SPA, 1)):
+        r = g.LdpcDecoder(code, algorithm=algo).decode_arrays(llr, 9, beliefs=True)
+        assert_same_decode(r, ocode.decode(llr, 9, algo=oalgo), code.k())
+    # early_stop = 0 runs every frame to max_iter
+    short = g.LdpcCode.dvb_t2_short(0)
+    r = g.LdpcDecoder(short, early_stop=False).decode_arrays(np.full((2, short.n()), 5.0, np.float32), 7)
+    assert (r["iters"] == 7).all() and r["conv"].all()
