@@ -137,18 +137,18 @@ __device__ void encode_frame(const DevCode& C, const uint32_t* u, uint32_t* cw, 
 static size_t encode_smem(const DevCode& C) {
   const int wn = (C.n + 31) / 32, wk = (C.k + 31) / 32, wm = (C.m + 31) / 32;
   const int scratch = std::max(wm + 64, 2 * C.words_m);
-  return (size_t)(wk + wn + scratch + 4) * 4;
+  return (size_t)(((wk + 3) & ~3) + ((wn + 3) & ~3) + scratch + 4) * 4;
 }
 
 __global__ void __launch_bounds__(kEncThreads) encode_kernel(const DevCode* __restrict__ Cp,
                                                              const uint64_t* __restrict__ msg,
                                                              long long frames, uint64_t* __restrict__ cw) {
-  extern __shared__ uint32_t sm[];
+  extern __shared__ __align__(16) uint32_t sm[];
   const DevCode C = *Cp;
   const int wn = (C.n + 31) / 32, wk = (C.k + 31) / 32;
   uint32_t* u = sm;
-  uint32_t* c = sm + wk;
-  uint32_t* scratch = c + wn;
+  uint32_t* c = sm + ((wk + 3) & ~3);  // 16-byte aligned carve-up (scratch holds u64 words)
+  uint32_t* scratch = c + ((wn + 3) & ~3);
   for (long long f = blockIdx.x; f < frames; f += gridDim.x) {
     const uint32_t* mi = (const uint32_t*)(msg + f * (long long)C.words_k);
     for (int w = threadIdx.x; w < wk; w += blockDim.x) {
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kEncThreads) encode_kernel(const DevCode* __re
 __global__ void __launch_bounds__(256) syndrome_kernel(const DevCode* __restrict__ Cp,
                                                        const uint64_t* __restrict__ cw, long long frames,
                                                        uint64_t* __restrict__ synd, int32_t* __restrict__ weight) {
-  extern __shared__ uint32_t sm[];
+  extern __shared__ __align__(16) uint32_t sm[];
   __shared__ int s_w;
   const DevCode C = *Cp;
   const int wn = (C.n + 31) / 32;
@@ -188,7 +188,9 @@ __global__ void __launch_bounds__(256) syndrome_kernel(const DevCode* __restrict
       }
       cnt += s;
       const uint32_t b = __ballot_sync(0xffffffffu, s);
-      if ((threadIdx.x & 31) == 0 && so) so[p >> 5] = b;
+      // a frame owns 2 * words_m 32-bit words; base is a multiple of 32, so lane
+      // 0 bounds the whole warp's word
+      if ((threadIdx.x & 31) == 0 && so && p < 64 * C.words_m) so[p >> 5] = b;
     }
     atomicAdd(&s_w, cnt);
     __syncthreads();
@@ -202,12 +204,12 @@ __global__ void __launch_bounds__(kEncThreads) channel_kernel(const DevCode* __r
                                                               const double* __restrict__ sigma2,
                                                               uint64_t* __restrict__ info,
                                                               uint64_t* __restrict__ cwo, float* __restrict__ llr) {
-  extern __shared__ uint32_t sm[];
+  extern __shared__ __align__(16) uint32_t sm[];
   const DevCode C = *Cp;
   const int wn = (C.n + 31) / 32, wk = (C.k + 31) / 32;
   uint32_t* u = sm;
-  uint32_t* c = sm + wk;
-  uint32_t* scratch = c + wn;
+  uint32_t* c = sm + ((wk + 3) & ~3);  // 16-byte aligned carve-up (scratch holds u64 words)
+  uint32_t* scratch = c + ((wn + 3) & ~3);
   for (long long f = blockIdx.x; f < frames; f += gridDim.x) {
     const uint32_t fr = (uint32_t)(frame0 + (unsigned long long)f);
     // info bits: 128 per Philox call, counter (block, frame, 1, 0)
