@@ -37,10 +37,14 @@ METRIC = "decoded info Gbit/s on 1 B200 at matched FER: learned min-sum vs plain
 UNIT = "Gbit/s"
 
 WORKLOADS = {
-    "c2": dict(frame=0, rate=1, frames=4096, algo=1, sched=1, msg16=True, max_iter=50,
+    "c2": dict(frame=0, rate=1, frames=4096, algo=3, sched=1, msg16=True, max_iter=50,
                ebn0=[0.6 + 0.1 * i for i in range(9)],
-               desc="dvbt2-normal-3/5 layered sum-product, fp16 messages / fp32 math, 4096 frames, "
+               desc="dvbt2-normal-3/5 layered sum-product (SFU), fp16 messages / fp32 math, 4096 frames, "
                     "Eb/N0 0.6..1.4 dB (frame f at 0.6+0.1*(f mod 9)), max 50 it, early stop"),
+    "c2exact": dict(frame=0, rate=1, frames=4096, algo=1, sched=1, msg16=True, max_iter=50,
+                    ebn0=[0.6 + 0.1 * i for i in range(9)],
+                    desc="dvbt2-normal-3/5 layered sum-product (bit-exact numerics), fp16 messages, "
+                         "4096 frames, Eb/N0 0.6..1.4 dB, max 50 it, early stop"),
     "c1": dict(frame=1, rate=0, frames=256, algo=1, sched=0, msg16=False, max_iter=50, ebn0=[1.0],
                desc="dvbt2-short-1/2 flooding sum-product fp32, 256 frames, Eb/N0 1.0 dB, max 50 it"),
     "c1ref": dict(frame=1, rate=0, frames=256, algo=0, sched=0, msg16=False, max_iter=50, ebn0=[1.0],

@@ -13,6 +13,7 @@ from .ldpc import (AwgnChannel, BpskModulator, CirculantMatrix, CodeRate, Decode
 ALGO_MINSUM = _capi.ALGO_MINSUM
 ALGO_SPA = _capi.ALGO_SPA
 ALGO_NMS = _capi.ALGO_NMS
+ALGO_SPA_FAST = _capi.ALGO_SPA_FAST
 SCHED_FLOODING = _capi.SCHED_FLOODING
 SCHED_LAYERED = _capi.SCHED_LAYERED
 MSG_F32 = _capi.MSG_F32
@@ -21,5 +22,5 @@ Gf2cError = _capi.Gf2cError
 
 __all__ = ["AwgnChannel", "BpskModulator", "CirculantMatrix", "CodeRate", "DecoderResult", "FrameSize", "Llr",
            "LdpcCode", "LdpcDecoder", "LdpcEncoder", "QuasiCyclicLdpc", "awgn_frames", "pack_bits",
-           "sigma2_from_ebn0", "unpack_bits", "words", "ALGO_MINSUM", "ALGO_SPA", "ALGO_NMS", "SCHED_FLOODING",
+           "sigma2_from_ebn0", "unpack_bits", "words", "ALGO_MINSUM", "ALGO_SPA", "ALGO_NMS", "ALGO_SPA_FAST", "SCHED_FLOODING",
            "SCHED_LAYERED", "MSG_F32", "MSG_F16", "Gf2cError"]

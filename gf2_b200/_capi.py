@@ -21,6 +21,7 @@ MEM_DEVICE = 1
 ALGO_MINSUM = 0
 ALGO_SPA = 1
 ALGO_NMS = 2
+ALGO_SPA_FAST = 3
 SCHED_FLOODING = 0
 SCHED_LAYERED = 1
 MSG_F32 = 0

@@ -58,8 +58,9 @@ struct gf2c_decoder {
   gf2c_decoder_opts opts{};
   int dev = 0;
   DevBuf d_codes;
-  int max_n = 0, max_words_k = 0, max_e_slots = 0, max_dc = 0, max_nchk = 0;
-  int dcmax = 0, threads = 0, grid = 0, bitmap_words = 0, smem_app_floats = 0;
+  int max_n = 0, max_m = 0, max_words_k = 0, max_e_slots = 0, max_dc = 0, max_nchk = 0;
+  int dcmax = 0, threads = 0, grid = 0, bitmap_words = 0, parity_words = 0, smem_app_floats = 0;
+  const void* kernel = nullptr;
   size_t smem = 0;
   long long work_stride = 0, app_offset = 0;
   DevBuf work, queue, status, alpha, beta;
@@ -275,7 +276,7 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   gf2c_decoder_opts o;
   if (opts) o = *opts;
   else gf2c_decoder_opts_default(&o);
-  if (o.algorithm < 0 || o.algorithm > 2 || o.schedule < 0 || o.schedule > 1 || o.msg_dtype < 0 ||
+  if (o.algorithm < 0 || o.algorithm > 3 || o.schedule < 0 || o.schedule > 1 || o.msg_dtype < 0 ||
       o.msg_dtype > 1 || o.threads_per_block < 0 || o.threads_per_block > 1024 || o.blocks_per_sm < 0 ||
       (o.threads_per_block % 32) != 0)
     return set_error(GF2C_ERR_INVALID_ARG, "invalid decoder options");
@@ -296,13 +297,17 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
     d->codes.push_back(codes[i]);
     dc.push_back(h.dev);
     d->max_n = std::max(d->max_n, (int)h.n);
+    d->max_m = std::max(d->max_m, (int)h.m);
     d->max_words_k = std::max(d->max_words_k, (int)((h.k + 63) / 64));
     d->max_e_slots = std::max(d->max_e_slots, h.e_slots);
     d->max_dc = std::max(d->max_dc, h.max_dc);
     d->max_nchk = std::max(d->max_nchk, h.max_nchk);
   }
-  d->dcmax = decode_dcmax_bucket(d->max_dc);
-  if (d->dcmax < 0) return set_error(GF2C_ERR_UNSUPPORTED, "check degree above 64");
+  const bool layered = o.schedule == GF2C_SCHED_LAYERED;
+  d->dcmax = layered ? layered_dcmax_bucket(d->max_dc) : decode_dcmax_bucket(d->max_dc);
+  if (d->dcmax < 0)
+    return set_error(GF2C_ERR_UNSUPPORTED, layered ? "layered schedule: check degree above 32"
+                                                   : "check degree above 64");
   int rc = d->d_codes.ensure(sizeof(DevCode) * dc.size());
   if (rc) return rc;
   GF2C_CUDA(cudaMemcpy(d->d_codes.p, dc.data(), sizeof(DevCode) * dc.size(), cudaMemcpyHostToDevice));
@@ -327,30 +332,35 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   int sms = 148;
   GF2C_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->dev));
   int threads = o.threads_per_block;
-  if (threads == 0) threads = (o.schedule == GF2C_SCHED_LAYERED) ? ((d->max_nchk + 31) / 32) * 32 : 512;
-  if (o.schedule == GF2C_SCHED_LAYERED && threads < d->max_nchk)
+  if (threads == 0) threads = layered ? ((d->max_nchk + 31) / 32) * 32 : 512;
+  if (layered && threads < d->max_nchk)
     return set_error(GF2C_ERR_INVALID_ARG, "layered schedule needs threads_per_block >= row group size");
   threads = std::max(threads, 32);
   d->threads = threads;
   d->bitmap_words = (d->max_n + 31) / 32;
-  const int app_floats = d->max_n;
-  size_t bm = decode_smem_bytes(0, d->bitmap_words);
-  d->smem_app_floats = (bm + (size_t)app_floats * 4 <= (size_t)kSmemBudget) ? app_floats : 0;
-  // a mixed batch may still keep its shorter codes in shared memory
-  if (d->smem_app_floats == 0) {
-    int best = 0;
-    for (auto* c : d->codes)
-      if (bm + (size_t)c->h->n * 4 <= (size_t)kSmemBudget) best = std::max(best, (int)c->h->n);
-    d->smem_app_floats = best;
-  }
-  d->smem = decode_smem_bytes(d->smem_app_floats, d->bitmap_words);
+  d->parity_words = layered ? (d->max_m + 31) / 32 : 0;
+  auto smem_of = [&](int app_floats) {
+    return layered ? layered_smem_bytes(app_floats, d->bitmap_words, d->parity_words)
+                   : decode_smem_bytes(app_floats, d->bitmap_words);
+  };
+  // keep the APP of every code whose n fits in shared memory there
+  d->smem_app_floats = 0;
+  for (auto* c : d->codes)
+    if (smem_of((int)c->h->n) <= (size_t)kSmemBudget) d->smem_app_floats = std::max(d->smem_app_floats, (int)c->h->n);
+  d->smem = smem_of(d->smem_app_floats);
   const size_t msg_bytes = o.msg_dtype == GF2C_MSG_F16 ? 2 : 4;
   const long long c2v_bytes = (((long long)d->max_e_slots * msg_bytes) + 255) / 256 * 256;
   d->app_offset = c2v_bytes;
   const bool need_gapp = d->max_n > d->smem_app_floats;
   d->work_stride = c2v_bytes + (need_gapp ? ((long long)d->max_n * 4 + 255) / 256 * 256 : 0);
+  d->kernel = layered ? layered_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax, threads)
+                      : flood_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax);
+  if (!d->kernel) return set_error(GF2C_ERR_UNSUPPORTED, "no decode kernel for this configuration");
+  if (!layered && threads > 512)
+    return set_error(GF2C_ERR_INVALID_ARG, "flooding schedule: threads_per_block must be <= 512");
+  GF2C_CUDA(cudaFuncSetAttribute(d->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d->smem));
   int occ = 0;
-  if ((rc = prepare_decode(o.algorithm, o.msg_dtype, o.schedule, d->dcmax, d->smem, threads, &occ))) return rc;
+  GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, d->kernel, threads, d->smem));
   if (occ <= 0) return set_error(GF2C_ERR_UNSUPPORTED, "decode kernel does not fit on an SM with this shape");
   int bps = o.blocks_per_sm ? std::min(o.blocks_per_sm, occ) : occ;
   d->grid = sms * bps;
@@ -387,6 +397,7 @@ static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaSt
   a.app_offset = d->app_offset;
   a.smem_app_floats = d->smem_app_floats;
   a.bitmap_words = d->bitmap_words;
+  a.parity_words = d->parity_words;
   a.alpha = (const float*)d->alpha.p;
   a.beta = (const float*)d->beta.p;
   a.nms_iters = d->opts.algorithm == GF2C_ALGO_NMS ? d->nms_iters : 0;
@@ -396,8 +407,9 @@ static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaSt
   GF2C_CUDA(cudaMemsetAsync(d->queue.p, 0, sizeof(unsigned long long), st));
   int grid = (int)std::min<int64_t>(d->grid, frames);
   d->last_launches = 1;
-  return launch_decode(d->opts.algorithm, d->opts.msg_dtype, d->opts.schedule, d->dcmax, a, grid,
-                       d->threads, d->smem, st);
+  void* args[] = {(void*)&a};
+  GF2C_CUDA(cudaLaunchKernel(d->kernel, dim3(grid), dim3(d->threads), args, d->smem, st));
+  return GF2C_OK;
 }
 
 static int check_status(gf2c_decoder* d, cudaStream_t st) {

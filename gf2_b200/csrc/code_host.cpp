@@ -46,6 +46,10 @@ static void finish_sparse(HostCode& c, std::vector<std::vector<int64_t>>& per_ro
   c.k = c.n > c.m ? c.n - c.m : 0;
 }
 
+static uint32_t pack_desc(int type, int base, int shift_or_q) {
+  return (uint32_t)base | ((uint32_t)shift_or_q << 20) | ((uint32_t)type << 30);
+}
+
 // Edge of (check, var) in CSR, -1 if absent.
 static int64_t find_edge(const HostCode& c, int64_t p, int64_t v) {
   auto b = c.row_idx.begin() + c.row_ptr[p], e = c.row_idx.begin() + c.row_ptr[p + 1];
@@ -92,6 +96,13 @@ static bool finish_plan(HostCode& c) {
   int nvg = (int)((c.n + c.vgs - 1) / c.vgs);
   c.vg.assign(nvg, int2{0, 0});
   c.vg_slot.clear();
+  c.vg_chk.clear();
+  std::vector<int> slot_cc(c.e_slots, -1);
+  for (size_t g = 0; g < c.cg.size(); g++) {
+    int4 G = c.cg[g];
+    for (int i = 0; i < G.z; i++)
+      for (int t = 0; t < G.y; t++) slot_cc[(size_t)G.w + (size_t)i * G.y + t] = G.x + t;
+  }
   c.max_dv = 0;
   for (int h = 0; h < nvg; h++) {
     int dv = 0;
@@ -103,12 +114,16 @@ static bool finish_plan(HostCode& c) {
     c.vg[h] = int2{dv, (int)c.vg_slot.size()};
     size_t base = c.vg_slot.size();
     c.vg_slot.resize(base + (size_t)dv * c.vgs, -1);
+    c.vg_chk.resize(base + (size_t)dv * c.vgs, -1);
     for (int j = 0; j < c.vgs; j++) {
       int64_t v = (int64_t)h * c.vgs + j;
       if (v >= c.n) break;
       int i = 0;
-      for (int64_t s = c.col_ptr[v]; s < c.col_ptr[v + 1]; s++, i++)
-        c.vg_slot[base + (size_t)i * c.vgs + j] = edge_slot[c.col_edge[s]];
+      for (int64_t s = c.col_ptr[v]; s < c.col_ptr[v + 1]; s++, i++) {
+        const int sl = edge_slot[c.col_edge[s]];
+        c.vg_slot[base + (size_t)i * c.vgs + j] = sl;
+        c.vg_chk[base + (size_t)i * c.vgs + j] = slot_cc[sl];
+      }
     }
     c.max_dv = std::max(c.max_dv, dv);
   }
@@ -199,6 +214,8 @@ int build_qc(const int32_t* base, int mb, int nb, int z, HostCode& c) {
     int dc = (int)circ.size();
     c.cg.push_back(int4{r * z, z, dc, edge0});
     c.cg_sync.push_back(0);
+    for (int i = 0; i < dc; i++) c.slot_desc.push_back(pack_desc(0, circ[i].first * z, circ[i].second));
+    c.cg_ninfo.push_back(dc);
     c.slot_var.resize((size_t)edge0 + (size_t)dc * z, -1);
     for (int t = 0; t < z; t++) {
       c.cg_checks.push_back((int64_t)r * z + t);
@@ -209,8 +226,12 @@ int build_qc(const int32_t* base, int mb, int nb, int z, HostCode& c) {
   }
   c.e_slots = edge0;
   c.vgs = z <= 1024 ? z : 256;
-  c.layered_ok = z <= 1024 ? 1 : 0;
-  if (!finish_plan(c)) plan_generic(c);
+  c.layered_ok = (z <= 1023 && c.n < (1 << 20)) ? 1 : 0;
+  if (!c.layered_ok) c.slot_desc.clear();
+  if (!finish_plan(c)) {
+    c.slot_desc.clear();
+    plan_generic(c);
+  }
   return GF2C_OK;
 }
 
@@ -261,6 +282,11 @@ int build_dvbt2(int frame, int rate, HostCode& c) {
     for (int i = 0; i + 1 < ninfo; i++)
       if (cl[i].first == cl[i + 1].first) sync |= 1u << i;
     c.cg_sync.push_back(sync);
+    for (int i = 0; i < ninfo; i++)
+      c.slot_desc.push_back(pack_desc(0, cl[i].first * (int)Z, (int)((Z - cl[i].second) % Z)));
+    c.slot_desc.push_back(pack_desc(1, (int)(k + a), (int)q));
+    c.slot_desc.push_back(pack_desc(2, (int)(k + a), (int)q));
+    c.cg_ninfo.push_back(ninfo);
     c.slot_var.resize((size_t)edge0 + (size_t)dc * Z, -1);
     for (int t = 0; t < Z; t++) {
       int64_t p = a + q * t;
@@ -276,7 +302,26 @@ int build_dvbt2(int frame, int rate, HostCode& c) {
   c.e_slots = edge0;
   c.vgs = (int)Z;
   c.layered_ok = 1;
-  if (!finish_plan(c)) plan_generic(c);
+  if (!finish_plan(c)) {
+    c.slot_desc.clear();
+    plan_generic(c);
+  }
+  // cross-check the descriptors against the slot table
+  for (size_t g = 0; g < c.cg.size() && !c.slot_desc.empty(); g++) {
+    const int4 G = c.cg[g];
+    for (int i = 0; i < G.z; i++) {
+      const uint32_t D = c.slot_desc[G.w / G.y + i];
+      const int type = (int)(D >> 30), sh = (int)((D >> 20) & 1023u), base = (int)(D & 0xFFFFFu);
+      for (int t = 0; t < G.y; t++) {
+        int v;
+        if (type == 0) v = base + (t + sh) % G.y;
+        else if (type == 1) v = (g == 0 && t == 0) ? -1 : base + sh * t - 1;
+        else v = base + sh * t;
+        if (v != c.slot_var[(size_t)G.w + (size_t)i * G.y + t])
+          return set_error(GF2C_ERR_KERNEL, "internal: DVB-T2 slot descriptor mismatch");
+      }
+    }
+  }
   return GF2C_OK;
 }
 
@@ -393,6 +438,10 @@ int upload_code(HostCode& c) {
     if ((rc = dev_copy(c, c.chk_cg, &d.chk_cg))) return rc;
     if ((rc = dev_copy(c, c.vg, &d.vg))) return rc;
     if ((rc = dev_copy(c, c.vg_slot, &d.vg_slot))) return rc;
+    if ((rc = dev_copy(c, c.vg_chk, &d.vg_chk))) return rc;
+    if ((rc = dev_copy(c, c.slot_desc, &d.slot_desc))) return rc;
+    if ((rc = dev_copy(c, c.slot_desc.empty() ? std::vector<int>() : c.cg_ninfo, &d.cg_ninfo))) return rc;
+    d.z = c.slot_desc.empty() ? 0 : c.z;
     std::vector<int> rp(c.row_ptr.begin(), c.row_ptr.end()), ri(c.row_idx.begin(), c.row_idx.end());
     if ((rc = dev_copy(c, rp, &d.csr_ptr))) return rc;
     if ((rc = dev_copy(c, ri, &d.csr_idx))) return rc;

@@ -1,4 +1,4 @@
-// gf2cuda decode kernels (sm_100a).
+// gf2cuda flooding-schedule decoder (sm_100a).
 //
 // One persistent kernel decodes a batch: each CTA takes the next frame from an
 // atomic queue, decodes it to completion (per-frame early stop, no wasted
@@ -9,19 +9,18 @@
 // the same workspace, laid out check-group-major so that consecutive threads
 // (consecutive checks of a circulant) touch consecutive addresses.
 //
-// Schedules
-//   flooding: LdpcDecoder::decode_iterative (crates/gf2-coding/src/ldpc/core.rs:889-938).
-//     The reference stores v2c and c2v; here only c2v and the belief are
-//     stored and v2c = belief - c2v is formed inside the check node, which is
-//     the same IEEE subtraction the reference performs (core.rs:831-836), so
-//     messages and beliefs agree bit for bit.  The belief sum runs over the
-//     variable's checks in ascending original check index (core.rs:824-827,
-//     the CSC order of sparse.rs:297-328).  The syndrome of iteration t is
-//     evaluated while the check nodes of iteration t+1 read the beliefs.
-//   layered (no reference counterpart): row group by row group, v2c from the
-//     pre-layer APP, APP += (c2v_new - c2v_old); a variable with several edges
-//     in one row group adds its deltas in ascending circulant shift, ordered by
-//     barriers between same-block slots.
+// Schedule: LdpcDecoder::decode_iterative (crates/gf2-coding/src/ldpc/core.rs:889-938).
+// The reference stores v2c and c2v; here only c2v and the belief are stored and
+// v2c = belief - c2v is formed inside the check node, which is the same IEEE
+// subtraction the reference performs (core.rs:831-836), so messages and beliefs
+// agree bit for bit.  The belief sum runs over the variable's checks in
+// ascending original check index (core.rs:824-827, the CSC order of
+// gf2-core/src/sparse.rs:297-328).  The syndrome of iteration t is evaluated
+// while the check nodes of iteration t+1 read the beliefs.
+//
+// Every check node first computes the variables of all its slots, then issues
+// all loads from always-valid addresses, then does the arithmetic, so the
+// loads of one check are in flight together.
 #include <cuda_fp16.h>
 
 #include "internal.h"
@@ -29,7 +28,23 @@
 
 namespace gf2c {
 
-enum { ALGO_MS = 0, ALGO_SPA = 1, ALGO_NMS = 2 };
+enum { ALGO_MS = 0, ALGO_SPA = 1, ALGO_NMS = 2, ALGO_SPA_FAST = 3 };
+
+__device__ __forceinline__ float sfu_ex2(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float sfu_lg2(float x) {
+  float r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float sfu_rcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 
 template <int DCMAX>
 struct MaskOf {
@@ -45,117 +60,181 @@ struct MaskOf<64> {
 struct FrameCtx {
   int n, m, k, ncg, vgs;
   const int4* cg;
-  const uint32_t* cg_sync;
   const int* slot_var;
+  const uint32_t* slot_desc;
   const uint16_t* chk_cg;
   const int2* vg;
   const int* vg_slot;
 };
 
-// Check-node update of one check (slots s0 + i*nchk, i < d).  Reads the current
-// APP and the old c2v, writes the new c2v.  Returns the parity of the hard
-// decisions of the APP over the check (the syndrome bit of the previous
-// iteration).  In the layered schedule the deltas are returned in delta[] and
-// the variable indices in var[].
-template <int ALGO, int MSG16, int DCMAX, bool LAYERED>
-__device__ __forceinline__ int check_update(const FrameCtx& F, int g, int s0, int nchk, int d,
-                                            const float* __restrict__ app,
-                                            typename MsgIO<MSG16>::T* __restrict__ c2v,
-                                            bool first, float al, float be, float* delta,
-                                            int* var) {
+__device__ __forceinline__ int desc_var(uint32_t D, int t, int Z, int g) {
+  const int base = (int)(D & 0xFFFFFu), sh = (int)((D >> 20) & 1023u), type = (int)(D >> 30);
+  if (type == 0) {
+    const int c = t + sh;
+    return base + (c >= Z ? c - Z : c);
+  }
+  const int v = base + sh * t;
+  if (type == 1) return (g == 0 && t == 0) ? -1 : v - 1;
+  return v;
+}
+
+// Check-node update of flattened check cc: reads the APP and the old c2v,
+// writes the new c2v.  Returns the parity of the hard decisions of the APP over
+// the check (the syndrome bit of the previous iteration).
+template <int ALGO, int MSG16, int DCMAX>
+__device__ __forceinline__ int check_update(const FrameCtx& F, int cc, const float* __restrict__ app,
+                                            typename MsgIO<MSG16>::T* __restrict__ c2v, bool first, float al,
+                                            float be) {
   typedef MsgIO<MSG16> IO;
   typedef typename MaskOf<DCMAX>::T MaskT;
+  const int g = F.chk_cg[cc];
+  const int4 G = F.cg[g];
+  const int t = cc - G.x, nchk = G.y, d = G.z, s0 = G.w + t;
+  int vv[DCMAX];
+  float ap[DCMAX], o[DCMAX];
+  if (F.slot_desc) {
+    const uint32_t* sd = F.slot_desc + G.w / nchk;
+#pragma unroll
+    for (int i = 0; i < DCMAX; i++) vv[i] = (i < d) ? desc_var(__ldg(&sd[i]), t, nchk, g) : -1;
+  } else {
+#pragma unroll
+    for (int i = 0; i < DCMAX; i++) vv[i] = (i < d) ? __ldg(&F.slot_var[s0 + i * nchk]) : -1;
+  }
+#pragma unroll
+  for (int i = 0; i < DCMAX; i++) ap[i] = app[vv[i] < 0 ? 0 : vv[i]];
+  if (first) {
+#pragma unroll
+    for (int i = 0; i < DCMAX; i++) o[i] = 0.0f;
+  } else {
+#pragma unroll
+    for (int i = 0; i < DCMAX; i++) o[i] = IO::ld(c2v, (i < d) ? s0 + i * nchk : s0);
+  }
   int par = 0;
   MaskT neg = 0, real = 0;
-  float old[DCMAX];
+#pragma unroll
+  for (int i = 0; i < DCMAX; i++) {
+    const bool r = vv[i] >= 0;
+    par ^= (int)(r && ap[i] < 0.0f);  // hard decision of the APP
+    ap[i] = __fsub_rn(ap[i], o[i]);   // v2c
+    real |= (MaskT)r << i;
+    neg |= (MaskT)(r && ap[i] < 0.0f) << i;
+  }
+  const int negp = MaskOf<DCMAX>::popc(neg) & 1;
+  const bool single = MaskOf<DCMAX>::popc(real) == 1;
   if (ALGO == ALGO_MS || ALGO == ALGO_NMS) {
-    float m1 = __int_as_float(0x7f800000), m2 = __int_as_float(0x7f800000);
+    float m1 = __int_as_float(0x7f800000), m2 = m1;
     int i1 = -1;
 #pragma unroll
     for (int i = 0; i < DCMAX; i++) {
-      var[i] = -1;
-      old[i] = 0.0f;
-      if (i < d) {
-        const int s = s0 + i * nchk;
-        const int v = __ldg(&F.slot_var[s]);
-        var[i] = v;
-        if (v >= 0) {
-          const float ap = app[v];
-          par ^= (ap < 0.0f);
-          const float o = first ? 0.0f : IO::ld(c2v, s);
-          old[i] = o;
-          const float x = __fsub_rn(ap, o);
-          const float ax = fabsf(x);
-          if (ax < m1) {
-            m2 = m1;
-            m1 = ax;
-            i1 = i;
-          } else if (ax < m2) {
-            m2 = ax;
-          }
-          neg |= (MaskT)(x < 0.0f) << i;
-          real |= (MaskT)1 << i;
-        }
+      const float ax = ((real >> i) & 1) ? fabsf(ap[i]) : __int_as_float(0x7f800000);
+      if (ax < m1) {
+        m2 = m1;
+        m1 = ax;
+        i1 = i;
+      } else if (ax < m2) {
+        m2 = ax;
       }
     }
-    const int negp = MaskOf<DCMAX>::popc(neg) & 1;
-    const bool single = MaskOf<DCMAX>::popc(real) == 1;
+    float mag1 = single ? 0.0f : m1, mag2 = single ? 0.0f : m2;
+    if (ALGO == ALGO_NMS) {
+      const float d1 = __fsub_rn(mag1, be), d2 = __fsub_rn(mag2, be);
+      mag1 = __fmul_rn(al, d1 > 0.0f ? d1 : 0.0f);
+      mag2 = __fmul_rn(al, d2 > 0.0f ? d2 : 0.0f);
+    }
 #pragma unroll
     for (int i = 0; i < DCMAX; i++) {
-      if (i < d && ((real >> i) & 1)) {
-        float mag = (i == i1) ? m2 : m1;
-        if (single) mag = 0.0f;
-        if (ALGO == ALGO_NMS) {
-          float dd = __fsub_rn(mag, be);
-          dd = dd > 0.0f ? dd : 0.0f;
-          mag = __fmul_rn(al, dd);
-        }
-        const int sg = negp ^ (int)((neg >> i) & 1);
-        const float out = sg ? -mag : mag;
-        IO::st(c2v, s0 + i * nchk, out);
-        if (LAYERED) delta[i] = __fsub_rn(IO::rt(out), old[i]);
+      if ((real >> i) & 1) {
+        const float mag = (i == i1) ? mag2 : mag1;
+        IO::st(c2v, s0 + i * nchk, (negp ^ (int)((neg >> i) & 1)) ? -mag : mag);
       }
     }
-  } else {  // sum-product
-    float tv[DCMAX];
+  } else if (ALGO == ALGO_SPA_FAST) {
+    // |c2v_i| = ln((D n_i + N d_i) / (D n_i - N d_i)), n = 1 - e, d = 1 + e, e = exp(-|x|)
+    float N = 1.0f, D = 1.0f;
 #pragma unroll
     for (int i = 0; i < DCMAX; i++) {
-      var[i] = -1;
-      old[i] = 0.0f;
-      tv[i] = 1.0f;
-      if (i < d) {
-        const int s = s0 + i * nchk;
-        const int v = __ldg(&F.slot_var[s]);
-        var[i] = v;
-        if (v >= 0) {
-          const float ap = app[v];
-          par ^= (ap < 0.0f);
-          const float o = first ? 0.0f : IO::ld(c2v, s);
-          old[i] = o;
-          tv[i] = tanh_half_f(__fsub_rn(ap, o));
-          real |= (MaskT)1 << i;
-        }
+      const float e = ((real >> i) & 1) ? sfu_ex2(fabsf(ap[i]) * -1.4426950408889634f) : 0.0f;
+      ap[i] = e;
+      N *= fmaxf(1.0f - e, 5.9604645e-08f);
+      D = __fmaf_rn(D, e, D);
+    }
+#pragma unroll
+    for (int i = 0; i < DCMAX; i++) {
+      if ((real >> i) & 1) {
+        const float ni = fmaxf(1.0f - ap[i], 5.9604645e-08f), di = 1.0f + ap[i];
+        const float num = __fmaf_rn(D, ni, N * di);
+        const float den = fmaxf(__fmaf_rn(D, ni, -N * di), num * 5.9604645e-08f);
+        float mag = 0.69314718055994531f * sfu_lg2(num * sfu_rcp(den));
+        mag = single ? 0.0f : fminf(mag, 16.635532f);
+        IO::st(c2v, s0 + i * nchk, (negp ^ (int)((neg >> i) & 1)) ? -mag : mag);
       }
     }
-    const bool single = MaskOf<DCMAX>::popc(real) == 1;
+  } else {  // sum-product with the library's exact numerics
     float suf[DCMAX];
+#pragma unroll
+    for (int i = 0; i < DCMAX; i++) ap[i] = ((real >> i) & 1) ? tanh_half_f(ap[i]) : 1.0f;
     suf[DCMAX - 1] = 1.0f;
 #pragma unroll
-    for (int i = DCMAX - 2; i >= 0; i--) suf[i] = (i + 1 < d) ? __fmul_rn(tv[i + 1], suf[i + 1]) : 1.0f;
+    for (int i = DCMAX - 2; i >= 0; i--) suf[i] = (i + 1 < d) ? __fmul_rn(ap[i + 1], suf[i + 1]) : 1.0f;
     float pre = 1.0f;
 #pragma unroll
     for (int i = 0; i < DCMAX; i++) {
-      if (i < d && ((real >> i) & 1)) {
+      if ((real >> i) & 1) {
         float p = __fmul_rn(pre, suf[i]);
         p = p > GF2C_SPA_PMAX ? GF2C_SPA_PMAX : (p < -GF2C_SPA_PMAX ? -GF2C_SPA_PMAX : p);
-        const float out = single ? 0.0f : two_atanh_f(p);
-        IO::st(c2v, s0 + i * nchk, out);
-        if (LAYERED) delta[i] = __fsub_rn(IO::rt(out), old[i]);
+        IO::st(c2v, s0 + i * nchk, single ? 0.0f : two_atanh_f(p));
       }
-      if (i < d) pre = (i == 0) ? tv[0] : __fmul_rn(pre, tv[i]);
+      if (i < d) pre = (i == 0) ? ap[0] : __fmul_rn(pre, ap[i]);
     }
   }
   return par;
+}
+
+// belief[v] = llr[v] + sum of c2v over v's checks in ascending original check
+// index, for two variables per thread with their slot and message loads
+// interleaved (4 slots per round).
+template <int MSG16>
+__device__ __forceinline__ void var_update2(const FrameCtx& F, int v0, int v1, const float* __restrict__ llr,
+                                            const typename MsgIO<MSG16>::T* __restrict__ c2v, float* app,
+                                            float& b0, float& b1) {
+  typedef MsgIO<MSG16> IO;
+  const int vgs = F.vgs;
+  int dv[2] = {0, 0};
+  const int* sl[2] = {F.vg_slot, F.vg_slot};
+  float b[2] = {0.0f, 0.0f};
+  const int vs[2] = {v0, v1};
+#pragma unroll
+  for (int u = 0; u < 2; u++) {
+    if (vs[u] >= 0) {
+      const int h = vs[u] / vgs, j = vs[u] - h * vgs;
+      const int2 V = F.vg[h];
+      dv[u] = V.x;
+      sl[u] = F.vg_slot + V.y + j;
+      b[u] = llr[vs[u]];
+    }
+  }
+  const int dmax = max(dv[0], dv[1]);
+  for (int i0 = 0; i0 < dmax; i0 += 4) {
+    int s[2][4];
+    float c[2][4];
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) s[u][q] = (i0 + q < dv[u]) ? __ldg(&sl[u][(i0 + q) * vgs]) : -1;
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) c[u][q] = IO::ld(c2v, s[u][q] < 0 ? 0 : s[u][q]);
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (s[u][q] >= 0) b[u] = __fadd_rn(b[u], c[u][q]);
+  }
+  if (v0 >= 0) app[v0] = b[0];
+  if (v1 >= 0) app[v1] = b[1];
+  b0 = b[0];
+  b1 = b[1];
 }
 
 // Parity of the hard decisions (from the bitmap) over all checks; block-wide OR.
@@ -175,8 +254,8 @@ __device__ __forceinline__ int syndrome_any(const FrameCtx& F, const uint32_t* b
   return __syncthreads_or(par);
 }
 
-template <int ALGO, int MSG16, int SCHED, int DCMAX>
-__global__ void __launch_bounds__(1024) bp_decode_kernel(const DecodeArgs a) {
+template <int ALGO, int MSG16, int DCMAX>
+__global__ void __launch_bounds__(512) bp_decode_kernel(const DecodeArgs a) {
   typedef MsgIO<MSG16> IO;
   typedef typename IO::T MsgT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -205,7 +284,7 @@ __global__ void __launch_bounds__(1024) bp_decode_kernel(const DecodeArgs a) {
     }
     if (tid == 0) C = a.codes[cid];
     __syncthreads();
-    FrameCtx F{C.n, C.m, C.k, C.ncg, C.vgs, C.cg, C.cg_sync, C.slot_var, C.chk_cg, C.vg, C.vg_slot};
+    FrameCtx F{C.n, C.m, C.k, C.ncg, C.vgs, C.cg, C.slot_var, C.slot_desc, C.chk_cg, C.vg, C.vg_slot};
     const int n = F.n;
     const float* __restrict__ llr = a.llr + (a.llr_off ? a.llr_off[f] : f * (long long)n);
     const int maxit = a.max_iter_arr ? a.max_iter_arr[f] : a.max_iter;
@@ -242,113 +321,42 @@ __global__ void __launch_bounds__(1024) bp_decode_kernel(const DecodeArgs a) {
     __syncthreads();
 
     int it = 0, converged = 0, synd = 1;
-    float delta[DCMAX];
-    int var[DCMAX];
-    if (SCHED == 0) {
-      for (;;) {
-        const int tw = (a.nms_iters > 0) ? min(it, a.nms_iters - 1) : 0;
-        int par = 0;
-        for (int cc = tid; cc < F.m; cc += NT) {
-          const int g = F.chk_cg[cc];
-          const int4 G = F.cg[g];
-          float al = 1.0f, be = 0.0f;
-          if (ALGO == ALGO_NMS) {
-            const int lay = (a.nms_L == F.ncg) ? g : 0;
-            al = a.alpha[tw * a.nms_L + lay];
-            be = a.beta[tw * a.nms_L + lay];
-          }
-          par |= check_update<ALGO, MSG16, DCMAX, false>(F, g, G.w + (cc - G.x), G.y, G.z, app, c2v,
-                                                         it == 0, al, be, delta, var);
+    for (;;) {
+      const int tw = (a.nms_iters > 0) ? min(it, a.nms_iters - 1) : 0;
+      int par = 0;
+      for (int cc = tid; cc < F.m; cc += NT) {
+        float al = 1.0f, be = 0.0f;
+        if (ALGO == ALGO_NMS) {
+          const int lay = (a.nms_L == F.ncg) ? (int)F.chk_cg[cc] : 0;
+          al = __ldg(&a.alpha[tw * a.nms_L + lay]);
+          be = __ldg(&a.beta[tw * a.nms_L + lay]);
         }
-        par = __syncthreads_or(par);
-        if (it > 0 && a.early_stop && !par) {
-          converged = 1;
-          synd = 0;
-          break;
-        }
-        // variable nodes: belief = llr + sum c2v, ascending original check index
-        for (int base = 0; base < n; base += NT) {
-          const int v = base + tid;
-          float b = 0.0f;
-          if (v < n) {
-            const int h = v / F.vgs;
-            const int j = v - h * F.vgs;
-            const int2 V = F.vg[h];
-            b = llr[v];
-            const int* sl = F.vg_slot + V.y + j;
-            for (int i = 0; i < V.x; i++) {
-              const int s = __ldg(&sl[i * F.vgs]);
-              if (s < 0) break;
-              b = __fadd_rn(b, IO::ld(c2v, s));
-            }
-            app[v] = b;
-          }
-          const unsigned bits = __ballot_sync(0xffffffffu, v < n && b < 0.0f);
-          if ((tid & 31) == 0 && v < n) bitmap[v >> 5] = bits;
-        }
-        __syncthreads();
-        ++it;
-        if (it >= maxit) break;
+        par |= check_update<ALGO, MSG16, DCMAX>(F, cc, app, c2v, it == 0, al, be);
       }
-      if (!converged) {
-        synd = syndrome_any(F, bitmap);
-        converged = !synd;
+      par = __syncthreads_or(par);
+      if (it > 0 && a.early_stop && !par) {
+        converged = 1;
+        synd = 0;
+        break;
       }
-    } else {
-      for (;;) {
-        const int tw = (a.nms_iters > 0) ? min(it, a.nms_iters - 1) : 0;
-        for (int g = 0; g < F.ncg; g++) {
-          const int4 G = F.cg[g];
-          const uint32_t sync = F.cg_sync[g];
-          const bool act = tid < G.y;
-          float al = 1.0f, be = 0.0f;
-          if (ALGO == ALGO_NMS) {
-            const int lay = (a.nms_L == F.ncg) ? g : 0;
-            al = a.alpha[tw * a.nms_L + lay];
-            be = a.beta[tw * a.nms_L + lay];
-          }
-          if (act)
-            check_update<ALGO, MSG16, DCMAX, true>(F, g, G.w + tid, G.y, G.z, app, c2v, it == 0, al,
-                                                   be, delta, var);
-          __syncthreads();
-          if (sync == 0) {
-            if (act) {
-#pragma unroll
-              for (int i = 0; i < DCMAX; i++) {
-                if (i < G.z && var[i] >= 0) {
-                  const int v = var[i];
-                  const float o = app[v];
-                  const float nw = __fadd_rn(o, delta[i]);
-                  app[v] = nw;
-                  if ((o < 0.0f) != (nw < 0.0f)) atomicXor(&bitmap[v >> 5], 1u << (v & 31));
-                }
-              }
-            }
-          } else {
-#pragma unroll
-            for (int i = 0; i < DCMAX; i++) {
-              if (i < G.z) {
-                if (act && var[i] >= 0) {
-                  const int v = var[i];
-                  const float o = app[v];
-                  const float nw = __fadd_rn(o, delta[i]);
-                  app[v] = nw;
-                  if ((o < 0.0f) != (nw < 0.0f)) atomicXor(&bitmap[v >> 5], 1u << (v & 31));
-                }
-                if ((sync >> i) & 1u) __syncthreads();
-              }
-            }
-          }
-          __syncthreads();
+      // variable nodes, two per thread per round
+      for (int base = 0; base < n; base += 2 * NT) {
+        const int v0 = base + tid, v1 = base + NT + tid;
+        float b0 = 0.0f, b1 = 0.0f;
+        var_update2<MSG16>(F, v0 < n ? v0 : -1, v1 < n ? v1 : -1, llr, c2v, app, b0, b1);
+        const unsigned m0 = __ballot_sync(0xffffffffu, v0 < n && b0 < 0.0f);
+        const unsigned m1 = __ballot_sync(0xffffffffu, v1 < n && b1 < 0.0f);
+        if ((tid & 31) == 0) {
+          if (v0 < n) bitmap[v0 >> 5] = m0;
+          if (v1 < n) bitmap[v1 >> 5] = m1;
         }
-        ++it;
-        synd = syndrome_any(F, bitmap);
-        if (a.early_stop && !synd) {
-          converged = 1;
-          break;
-        }
-        if (it >= maxit) break;
       }
+      __syncthreads();
+      ++it;
+      if (it >= maxit) break;
+    }
+    if (!converged) {
+      synd = syndrome_any(F, bitmap);
       converged = !synd;
     }
 
@@ -387,49 +395,27 @@ size_t decode_smem_bytes(int smem_app_floats, int bitmap_words) {
   return (size_t)((bitmap_words * 4 + 15) & ~15) + (size_t)smem_app_floats * 4;
 }
 
-template <int ALGO, int MSG16, int SCHED>
+template <int ALGO, int MSG16>
 static const void* kernel_dc(int dcmax) {
   switch (dcmax) {
-    case 8: return (const void*)bp_decode_kernel<ALGO, MSG16, SCHED, 8>;
-    case 16: return (const void*)bp_decode_kernel<ALGO, MSG16, SCHED, 16>;
-    case 24: return (const void*)bp_decode_kernel<ALGO, MSG16, SCHED, 24>;
-    case 32: return (const void*)bp_decode_kernel<ALGO, MSG16, SCHED, 32>;
-    case 64: return (const void*)bp_decode_kernel<ALGO, MSG16, SCHED, 64>;
+    case 8: return (const void*)bp_decode_kernel<ALGO, MSG16, 8>;
+    case 16: return (const void*)bp_decode_kernel<ALGO, MSG16, 16>;
+    case 24: return (const void*)bp_decode_kernel<ALGO, MSG16, 24>;
+    case 32: return (const void*)bp_decode_kernel<ALGO, MSG16, 32>;
+    case 64: return (const void*)bp_decode_kernel<ALGO, MSG16, 64>;
   }
   return nullptr;
 }
 
-template <int ALGO, int MSG16>
-static const void* kernel_sched(int sched, int dcmax) {
-  return sched == 0 ? kernel_dc<ALGO, MSG16, 0>(dcmax) : kernel_dc<ALGO, MSG16, 1>(dcmax);
-}
-
-const void* decode_kernel_ptr(int algo, int msg16, int sched, int dcmax) {
-  if (algo == ALGO_MS) return msg16 ? kernel_sched<ALGO_MS, 1>(sched, dcmax) : kernel_sched<ALGO_MS, 0>(sched, dcmax);
-  if (algo == ALGO_SPA)
-    return msg16 ? kernel_sched<ALGO_SPA, 1>(sched, dcmax) : kernel_sched<ALGO_SPA, 0>(sched, dcmax);
-  return msg16 ? kernel_sched<ALGO_NMS, 1>(sched, dcmax) : kernel_sched<ALGO_NMS, 0>(sched, dcmax);
-}
-
-int prepare_decode(int algo, int msg16, int sched, int dcmax, size_t smem, int threads, int* blocks_per_sm) {
-  const void* k = decode_kernel_ptr(algo, msg16, sched, dcmax);
-  if (!k) return set_error(GF2C_ERR_UNSUPPORTED, "no decode kernel for this configuration");
-  GF2C_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  if (blocks_per_sm) {
-    int b = 0;
-    GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, threads, smem));
-    *blocks_per_sm = b;
+// Flooding-schedule kernel for (algorithm, message type, degree bucket).
+const void* flood_kernel_ptr(int algo, int msg16, int dcmax) {
+  switch (algo) {
+    case ALGO_MS: return msg16 ? kernel_dc<ALGO_MS, 1>(dcmax) : kernel_dc<ALGO_MS, 0>(dcmax);
+    case ALGO_SPA: return msg16 ? kernel_dc<ALGO_SPA, 1>(dcmax) : kernel_dc<ALGO_SPA, 0>(dcmax);
+    case ALGO_NMS: return msg16 ? kernel_dc<ALGO_NMS, 1>(dcmax) : kernel_dc<ALGO_NMS, 0>(dcmax);
+    case ALGO_SPA_FAST: return msg16 ? kernel_dc<ALGO_SPA_FAST, 1>(dcmax) : kernel_dc<ALGO_SPA_FAST, 0>(dcmax);
   }
-  return GF2C_OK;
-}
-
-int launch_decode(int algo, int msg16, int sched, int dcmax, const DecodeArgs& a, int grid, int threads,
-                  size_t smem, cudaStream_t st) {
-  const void* k = decode_kernel_ptr(algo, msg16, sched, dcmax);
-  if (!k) return set_error(GF2C_ERR_UNSUPPORTED, "no decode kernel for this configuration");
-  void* args[] = {(void*)&a};
-  GF2C_CUDA(cudaLaunchKernel(k, dim3(grid), dim3(threads), args, smem, st));
-  return GF2C_OK;
+  return nullptr;
 }
 
 }  // namespace gf2c

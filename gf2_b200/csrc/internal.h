@@ -40,6 +40,15 @@ struct DevCode {
   const uint16_t* chk_cg;          // [m] flattened check -> CG
   const int2* vg;                  // {dv, vedge0}
   const int* vg_slot;              // VG-major, [vg][i][j]
+  const int* vg_chk;               // same layout: flattened check index of the edge
+  // QC / DVB-T2 codes: slot i of check group g is described by slot_desc[edge0/Z + i]
+  // (all Z checks of a row group share it), packed as base | shift_or_q << 20 | type << 30:
+  //   type 0 circulant:   var = base + (t + shift) mod Z
+  //   type 1 staircase sub-diagonal: var = base + q t - 1, absent for (row group 0, t 0)
+  //   type 2 staircase diagonal:     var = base + q t
+  const uint32_t* slot_desc;       // nullptr for codes without the QC structure
+  const int* cg_ninfo;             // per CG: number of circulant slots (the rest are staircase)
+  int z;                           // circulant size of slot_desc codes
   const int* csr_ptr;              // natural order H (m + 1)
   const int* csr_idx;              // (nnz)
   // encoder
@@ -68,6 +77,9 @@ struct HostCode {
   std::vector<uint16_t> chk_cg;
   std::vector<int2> vg;
   std::vector<int> vg_slot;
+  std::vector<int> vg_chk;
+  std::vector<uint32_t> slot_desc;         // QC / DVB-T2 slot descriptors (see DevCode)
+  std::vector<int> cg_ninfo;               // circulant slots per CG
   int vgs = 0, max_dc = 0, max_dv = 0, e_slots = 0, layered_ok = 0, max_nchk = 0;
   std::vector<int64_t> cg_checks;          // original check of each flattened check
 
@@ -139,6 +151,7 @@ struct DecodeArgs {
   long long app_offset;            // offset of the global APP inside a CTA workspace
   int smem_app_floats;             // APP kept in shared memory when n <= this
   int bitmap_words;                // 32-bit words of the hard-decision bitmap
+  int parity_words;                // 32-bit words of the check-parity bitmap (layered)
   const float* alpha;              // NMS weights [nms_iters][nms_L]
   const float* beta;
   int nms_iters;
@@ -147,11 +160,11 @@ struct DecodeArgs {
   int* status;                     // kernel-side error flag
 };
 
-int launch_decode(int algo, int msg16, int sched, int dcmax, const DecodeArgs& a, int grid,
-                  int threads, size_t smem, cudaStream_t st);
-int prepare_decode(int algo, int msg16, int sched, int dcmax, size_t smem, int threads,
-                   int* blocks_per_sm);
+const void* flood_kernel_ptr(int algo, int msg16, int dcmax);
 int decode_dcmax_bucket(int max_dc);
+int layered_dcmax_bucket(int max_dc);
+const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt);
+size_t layered_smem_bytes(int smem_app_floats, int bitmap_words, int parity_words);
 size_t decode_smem_bytes(int smem_app_floats, int bitmap_words);
 
 int launch_syndrome(const DevCode* dcode, const DevCode& hcode, const uint64_t* cw, long long frames,

@@ -1,0 +1,428 @@
+// gf2cuda layered-schedule decoder (sm_100a).
+//
+// The layered schedule has no counterpart in the reference (its decoder is the
+// flooding loop of crates/gf2-coding/src/ldpc/core.rs:889-938; layered decoding
+// is listed as future work in crates/gf2-coding/docs/LDPC_PERFORMANCE.md).  Row
+// groups of a QC / DVB-T2 code are processed in order; inside a row group every
+// check reads v2c = APP - c2v_old from the pre-layer APP, computes c2v_new and
+// adds (c2v_new - c2v_old) to the APP of its variables.
+//
+// One CTA decodes one frame at a time (persistent, frames from an atomic
+// queue), one thread per check of the row group.  The variable of every slot is
+// computed from a per-row-group slot descriptor shared by all checks (circulant
+// base + (t + shift) mod Z, or the DVB-T2 staircase), so no index table is read
+// in the hot loop.  All loads of a check are issued back to back from
+// always-valid addresses before any arithmetic (memory-level parallelism), and
+// then the check node, the message stores and the APP updates follow.
+//
+// A row group whose variables are all distinct writes the new APP directly
+// from the thread that read it (one barrier per row group); a row group with
+// repeated variables (DVB-T2 blocks holding several circulants) applies its
+// deltas slot by slot with a barrier between slots of the same block, i.e. in
+// ascending circulant shift.
+//
+// Early stop: instead of a syndrome pass per iteration, the kernel keeps the
+// parity of every check of the current hard decisions in shared memory and
+// the number of unsatisfied checks; a variable whose hard decision flips
+// toggles the parity of its checks.  The count is exact, so "count == 0 at
+// the end of an iteration" is the reference's syndrome test (core.rs:918-922).
+//
+// Check-node rules: min-sum / normalised-offset min-sum / sum-product with the
+// exact library numerics (bit-identical to the CPU restatement), and a fast
+// sum-product (GF2C_ALGO_SPA_FAST) evaluated with the SFU: e = 2^(-|x| log2 e),
+// n = 1 - e, d = 1 + e, N = prod n, D = prod d, and for edge i
+//   |c2v_i| = ln((D n_i + N d_i) / (D n_i - N d_i)) = 2 atanh(prod_{j != i} tanh(|x_j| / 2))
+// (three SFU operations per edge, no per-edge division of the products); its
+// APP update is v2c + c2v_new.
+#include <cuda_fp16.h>
+
+#include "internal.h"
+#include "numeric.cuh"
+
+namespace gf2c {
+
+enum { L_MS = 0, L_SPA = 1, L_NMS = 2, L_SPA_FAST = 3 };
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float lg2_approx(float x) {
+  float r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+template <int MSG16>
+__device__ __forceinline__ float ld_msg(const typename MsgIO<MSG16>::T* p, int s);
+template <>
+__device__ __forceinline__ float ld_msg<0>(const float* p, int s) { return __ldcs(p + s); }
+template <>
+__device__ __forceinline__ float ld_msg<1>(const __half* p, int s) {
+  return __half2float(__ushort_as_half(__ldcs((const unsigned short*)p + s)));
+}
+template <int MSG16>
+__device__ __forceinline__ void st_msg(typename MsgIO<MSG16>::T* p, int s, float v);
+template <>
+__device__ __forceinline__ void st_msg<0>(float* p, int s, float v) { __stcs(p + s, v); }
+template <>
+__device__ __forceinline__ void st_msg<1>(__half* p, int s, float v) {
+  __stcs((unsigned short*)p + s, __half_as_ushort(__float2half_rn(v)));
+}
+
+struct LayerSmem {
+  uint32_t* bitmap;   // hard decisions, n bits
+  uint32_t* chkpar;   // parity of each (flattened) check, m bits
+  int* unsat;         // number of unsatisfied checks
+};
+
+// Variable of packed slot descriptor D for check t of row group g (Z checks).
+__device__ __forceinline__ int slot_var_of(uint32_t D, int t, int Z, int g) {
+  const int base = (int)(D & 0xFFFFFu), sh = (int)((D >> 20) & 1023u), type = (int)(D >> 30);
+  if (type == 0) {
+    const int c = t + sh;
+    return base + (c >= Z ? c - Z : c);
+  }
+  const int v = base + sh * t;
+  if (type == 1) return (g == 0 && t == 0) ? -1 : v - 1;
+  return v;
+}
+
+// A hard decision flipped: toggle it and the parity of the variable's checks,
+// and update the number of unsatisfied checks (rare after the first iterations).
+__device__ __noinline__ void flip_var(int v, const LayerSmem S, const int2* __restrict__ vg,
+                                      const int* __restrict__ vg_chk, int vgs) {
+  atomicXor(&S.bitmap[v >> 5], 1u << (v & 31));
+  const int h = v / vgs, j = v - h * vgs;
+  const int2 V = vg[h];
+  int delta = 0;
+  for (int i = 0; i < V.x; i++) {
+    const int cc = __ldg(&vg_chk[V.y + i * vgs + j]);
+    if (cc < 0) break;
+    const uint32_t was = atomicXor(&S.chkpar[cc >> 5], 1u << (cc & 31));
+    delta += ((was >> (cc & 31)) & 1u) ? -1 : 1;
+  }
+  atomicAdd(S.unsat, delta);
+}
+
+__device__ __forceinline__ void app_put(float* app, int v, bool old_neg, float nw, const LayerSmem& S,
+                                        const int2* __restrict__ vg, const int* __restrict__ vg_chk, int vgs) {
+  app[v] = nw;
+  if (old_neg != (nw < 0.0f)) flip_var(v, S, vg, vg_chk, vgs);
+}
+
+template <int ALGO, int MSG16, int DCMAX, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs a) {
+  typedef typename MsgIO<MSG16>::T MsgT;
+  typedef MsgIO<MSG16> IO;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ long long s_frame;
+  __shared__ int s_unsat;
+  __shared__ DevCode C;
+  uint32_t* bitmap = (uint32_t*)smem_raw;
+  uint32_t* chkpar = bitmap + a.bitmap_words;
+  float* smem_app = (float*)(smem_raw + (((a.bitmap_words + a.parity_words) * 4 + 15) & ~15));
+  char* work = a.work + (long long)blockIdx.x * a.work_stride;
+  MsgT* __restrict__ c2v = (MsgT*)work;
+  float* gapp = (float*)(work + a.app_offset);
+  const int tid = threadIdx.x, NT = blockDim.x;
+  LayerSmem S{bitmap, chkpar, &s_unsat};
+
+  for (;;) {
+    if (tid == 0) {
+      s_frame = (long long)atomicAdd(a.queue, 1ull);
+      s_unsat = 0;
+    }
+    __syncthreads();
+    const long long f = s_frame;
+    if (f >= a.frames) break;
+    const int cid = a.code_id ? a.code_id[f] : 0;
+    if (cid < 0 || cid >= a.ncodes) {
+      if (tid == 0) {
+        atomicExch(a.status, 1);
+        if (a.iters) a.iters[f] = -1;
+      }
+      __syncthreads();
+      continue;
+    }
+    if (tid == 0) C = a.codes[cid];
+    __syncthreads();
+    const int n = C.n, m = C.m, vgs = C.vgs, ncg = C.ncg;
+    const int4* __restrict__ cgp = C.cg;
+    const uint32_t* __restrict__ cgs = C.cg_sync;
+    const int* __restrict__ slot_var = C.slot_var;
+    const uint32_t* __restrict__ sdesc = C.slot_desc;
+    const int2* __restrict__ vg = C.vg;
+    const int* __restrict__ vg_chk = C.vg_chk;
+    const float* __restrict__ llr = a.llr + (a.llr_off ? a.llr_off[f] : f * (long long)n);
+    const int maxit = a.max_iter_arr ? a.max_iter_arr[f] : a.max_iter;
+    float* app = (n <= a.smem_app_floats) ? smem_app : gapp;
+    uint64_t* mo = a.msg ? a.msg + (a.msg_off ? a.msg_off[f] : f * (long long)C.words_k) : nullptr;
+    float* bo = a.beliefs ? a.beliefs + (a.llr_off ? a.llr_off[f] : f * (long long)n) : nullptr;
+
+    if (maxit <= 0) {
+      if (mo)
+        for (int w = tid; w < C.words_k; w += NT) mo[w] = 0ull;
+      if (bo)
+        for (int v = tid; v < n; v += NT) bo[v] = 0.0f;
+      if (tid == 0) {
+        if (a.iters) a.iters[f] = 0;
+        if (a.conv) a.conv[f] = 0;
+        if (a.synd_ok) a.synd_ok[f] = 1;
+      }
+      __syncthreads();
+      continue;
+    }
+
+    // APP = llr; hard decisions
+    for (int base = 0; base < n; base += NT) {
+      const int v = base + tid;
+      float x = 0.0f;
+      if (v < n) {
+        x = __ldcs(llr + v);
+        app[v] = x;
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, v < n && x < 0.0f);
+      if ((tid & 31) == 0 && v < n) bitmap[v >> 5] = b;
+    }
+    __syncthreads();
+    // check parities and the unsatisfied count
+    {
+      int cnt = 0;
+      for (int base = 0; base < m; base += NT) {
+        const int cc = base + tid;
+        uint32_t p = 0;
+        if (cc < m) {
+          const int g = C.chk_cg[cc];
+          const int4 G = cgp[g];
+          const int t = cc - G.x;
+          for (int i = 0; i < G.z; i++) {
+            const int v = __ldg(&slot_var[G.w + i * G.y + t]);
+            if (v >= 0) p ^= (bitmap[v >> 5] >> (v & 31)) & 1u;
+          }
+        }
+        cnt += (int)p;
+        const unsigned b = __ballot_sync(0xffffffffu, p);
+        if ((tid & 31) == 0 && cc < m) chkpar[cc >> 5] = b;
+      }
+      atomicAdd(&s_unsat, cnt);
+    }
+    __syncthreads();
+
+    int it = 0, converged = 0;
+    for (;;) {
+      const int tw = (a.nms_iters > 0) ? min(it, a.nms_iters - 1) : 0;
+      const bool first = (it == 0);
+      for (int g = 0; g < ncg; g++) {
+        const int4 G = cgp[g];
+        const uint32_t sync = cgs[g];
+        const bool act = tid < G.y;
+        const int d = G.z, nchk = G.y;
+        const int t = act ? tid : 0;
+        const int s0 = G.w + t;
+        const uint32_t* __restrict__ sd = sdesc + G.w / nchk;
+        int vv[DCMAX];
+        float ap[DCMAX], o[DCMAX], w[DCMAX];
+        uint32_t real = 0, neg = 0, apneg = 0;
+        if (act) {
+          // 1. indices, 2. all loads, 3. arithmetic
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) vv[i] = (i < d) ? slot_var_of(__ldg(&sd[i]), t, nchk, g) : -1;
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) ap[i] = app[vv[i] < 0 ? 0 : vv[i]];
+          if (first) {
+#pragma unroll
+            for (int i = 0; i < DCMAX; i++) o[i] = 0.0f;
+          } else {
+#pragma unroll
+            for (int i = 0; i < DCMAX; i++) o[i] = ld_msg<MSG16>(c2v, (i < d) ? s0 + i * nchk : s0);
+          }
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) {
+            const bool r = vv[i] >= 0;
+            w[i] = __fsub_rn(ap[i], o[i]);  // v2c
+            real |= (uint32_t)r << i;
+            neg |= (uint32_t)(r && w[i] < 0.0f) << i;
+            apneg |= (uint32_t)(ap[i] < 0.0f) << i;
+          }
+          const int negp = __popc(neg) & 1;
+          const bool single = __popc(real) == 1;
+          if (ALGO == L_MS || ALGO == L_NMS) {
+            float m1 = __int_as_float(0x7f800000), m2 = m1;
+            int i1 = -1;
+#pragma unroll
+            for (int i = 0; i < DCMAX; i++) {
+              const float ax = ((real >> i) & 1u) ? fabsf(w[i]) : __int_as_float(0x7f800000);
+              if (ax < m1) {
+                m2 = m1;
+                m1 = ax;
+                i1 = i;
+              } else if (ax < m2) {
+                m2 = ax;
+              }
+            }
+            float mag1 = single ? 0.0f : m1, mag2 = single ? 0.0f : m2;
+            if (ALGO == L_NMS) {
+              const int lay = (a.nms_L == ncg) ? g : 0;
+              const float al = __ldg(&a.alpha[tw * a.nms_L + lay]);
+              const float be = __ldg(&a.beta[tw * a.nms_L + lay]);
+              const float d1 = __fsub_rn(mag1, be), d2 = __fsub_rn(mag2, be);
+              mag1 = __fmul_rn(al, d1 > 0.0f ? d1 : 0.0f);
+              mag2 = __fmul_rn(al, d2 > 0.0f ? d2 : 0.0f);
+            }
+#pragma unroll
+            for (int i = 0; i < DCMAX; i++) {
+              const float mag = (i == i1) ? mag2 : mag1;
+              w[i] = (negp ^ ((neg >> i) & 1u)) ? -mag : mag;
+            }
+          } else if (ALGO == L_SPA) {
+            float suf[DCMAX];
+#pragma unroll
+            for (int i = 0; i < DCMAX; i++) w[i] = ((real >> i) & 1u) ? tanh_half_f(w[i]) : 1.0f;
+            suf[DCMAX - 1] = 1.0f;
+#pragma unroll
+            for (int i = DCMAX - 2; i >= 0; i--) suf[i] = (i + 1 < d) ? __fmul_rn(w[i + 1], suf[i + 1]) : 1.0f;
+            float pre = 1.0f;
+#pragma unroll
+            for (int i = 0; i < DCMAX; i++) {
+              float p = __fmul_rn(pre, suf[i]);
+              p = p > GF2C_SPA_PMAX ? GF2C_SPA_PMAX : (p < -GF2C_SPA_PMAX ? -GF2C_SPA_PMAX : p);
+              const float out = single ? 0.0f : two_atanh_f(p);
+              if (i < d) pre = (i == 0) ? w[0] : __fmul_rn(pre, w[i]);
+              w[i] = out;
+            }
+          } else {  // fast sum-product; ap[] keeps v2c for the APP update
+            float N = 1.0f, Dp = 1.0f;
+#pragma unroll
+            for (int i = 0; i < DCMAX; i++) {
+              const float x = w[i];
+              ap[i] = x;
+              const float e = ((real >> i) & 1u) ? ex2_approx(fabsf(x) * -1.4426950408889634f) : 0.0f;
+              w[i] = e;
+              N *= fmaxf(1.0f - e, 5.9604645e-08f);
+              Dp = __fmaf_rn(Dp, e, Dp);
+            }
+#pragma unroll
+            for (int i = 0; i < DCMAX; i++) {
+              const float ni = fmaxf(1.0f - w[i], 5.9604645e-08f), di = 1.0f + w[i];
+              const float num = __fmaf_rn(Dp, ni, N * di);
+              const float den = fmaxf(__fmaf_rn(Dp, ni, -N * di), num * 5.9604645e-08f);
+              float mag = 0.69314718055994531f * lg2_approx(num * rcp_approx(den));
+              mag = single ? 0.0f : fminf(mag, 16.635532f);
+              w[i] = (negp ^ ((neg >> i) & 1u)) ? -mag : mag;
+            }
+          }
+          // message stores; APP update for row groups without repeated variables
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) {
+            if ((real >> i) & 1u) {
+              const float out = IO::rt(w[i]);
+              st_msg<MSG16>(c2v, s0 + i * nchk, out);
+              if (ALGO == L_SPA_FAST) {
+                if (sync == 0) app_put(app, vv[i], (apneg >> i) & 1u, ap[i] + out, S, vg, vg_chk, vgs);
+                else w[i] = out - o[i];
+              } else {
+                w[i] = __fsub_rn(out, o[i]);  // delta
+                if (sync == 0) app_put(app, vv[i], (apneg >> i) & 1u, __fadd_rn(ap[i], w[i]), S, vg, vg_chk, vgs);
+              }
+            }
+          }
+        }
+        if (sync != 0) {
+          __syncthreads();  // all pre-layer APP reads done
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) {
+            if (i < d) {
+              if (act && ((real >> i) & 1u)) {
+                const int v = vv[i];
+                const float ov = app[v];
+                app_put(app, v, ov < 0.0f, __fadd_rn(ov, w[i]), S, vg, vg_chk, vgs);
+              }
+              if ((sync >> i) & 1u) __syncthreads();
+            }
+          }
+        }
+        __syncthreads();
+      }
+      ++it;
+      const int unsat = s_unsat;
+      if (a.early_stop && unsat == 0) {
+        converged = 1;
+        break;
+      }
+      if (it >= maxit) break;
+      __syncthreads();  // s_unsat read by all before the next iteration's updates
+    }
+    if (!converged) converged = (s_unsat == 0);
+
+    if (mo) {
+      const int wn = (n + 31) >> 5;
+      for (int w = tid; w < C.words_k; w += NT) {
+        const uint32_t lo = bitmap[2 * w];
+        const uint32_t hi = (2 * w + 1 < wn) ? bitmap[2 * w + 1] : 0u;
+        unsigned long long word = (unsigned long long)lo | ((unsigned long long)hi << 32);
+        const int rem = C.k - 64 * w;
+        if (rem < 64) word &= (1ull << rem) - 1ull;
+        mo[w] = word;
+      }
+    }
+    if (bo)
+      for (int v = tid; v < n; v += NT) bo[v] = app[v];
+    if (tid == 0) {
+      if (a.iters) a.iters[f] = it;
+      if (a.conv) a.conv[f] = (uint8_t)converged;
+      if (a.synd_ok) a.synd_ok[f] = (uint8_t)converged;
+    }
+    __syncthreads();
+  }
+}
+
+template <int ALGO, int MSG16, int MAXT, int MINB>
+static const void* lay_dc(int dcmax) {
+  switch (dcmax) {
+    case 8: return (const void*)bp_layered_kernel<ALGO, MSG16, 8, MAXT, MINB>;
+    case 12: return (const void*)bp_layered_kernel<ALGO, MSG16, 12, MAXT, MINB>;
+    case 16: return (const void*)bp_layered_kernel<ALGO, MSG16, 16, MAXT, MINB>;
+    case 24: return (const void*)bp_layered_kernel<ALGO, MSG16, 24, MAXT, MINB>;
+    case 32: return (const void*)bp_layered_kernel<ALGO, MSG16, 32, MAXT, MINB>;
+  }
+  return nullptr;
+}
+
+template <int ALGO, int MSG16>
+static const void* lay_t(int dcmax, int maxt) {
+  if (maxt <= 384)
+    return ALGO == L_SPA ? lay_dc<ALGO, MSG16, 384, 1>(dcmax) : lay_dc<ALGO, MSG16, 384, 2>(dcmax);
+  return lay_dc<ALGO, MSG16, 1024, 1>(dcmax);
+}
+
+int layered_dcmax_bucket(int max_dc) {
+  if (max_dc <= 8) return 8;
+  if (max_dc <= 12) return 12;
+  if (max_dc <= 16) return 16;
+  if (max_dc <= 24) return 24;
+  if (max_dc <= 32) return 32;
+  return -1;
+}
+
+const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt) {
+  switch (algo) {
+    case L_MS: return msg16 ? lay_t<L_MS, 1>(dcmax, maxt) : lay_t<L_MS, 0>(dcmax, maxt);
+    case L_SPA: return msg16 ? lay_t<L_SPA, 1>(dcmax, maxt) : lay_t<L_SPA, 0>(dcmax, maxt);
+    case L_NMS: return msg16 ? lay_t<L_NMS, 1>(dcmax, maxt) : lay_t<L_NMS, 0>(dcmax, maxt);
+    case L_SPA_FAST: return msg16 ? lay_t<L_SPA_FAST, 1>(dcmax, maxt) : lay_t<L_SPA_FAST, 0>(dcmax, maxt);
+  }
+  return nullptr;
+}
+
+size_t layered_smem_bytes(int smem_app_floats, int bitmap_words, int parity_words) {
+  return (size_t)(((bitmap_words + parity_words) * 4 + 15) & ~15) + (size_t)smem_app_floats * 4;
+}
+
+}  // namespace gf2c

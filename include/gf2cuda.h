@@ -70,6 +70,9 @@ extern "C" {
                                llr.rs:210-215), FP32, |extrinsic product| <= 1 - 2^-23 */
 #define GF2C_ALGO_NMS 2     /* normalised + offset min-sum (llr.rs:352-399) with one
                                (alpha, beta) per iteration and row group */
+#define GF2C_ALGO_SPA_FAST 3 /* sum-product evaluated with the SFU (ex2/lg2/rcp approximations):
+                               2 atanh(prod tanh) through products of 1 -/+ e^-|x|; judged by
+                               FER and LLR deviation against the FP64 sum-product, not bit-exact */
 #define GF2C_SCHED_FLOODING 0  /* decode_iterative's schedule (core.rs:909-924) */
 #define GF2C_SCHED_LAYERED 1   /* row-group layered schedule (QC and DVB-T2 codes) */
 #define GF2C_MSG_F32 0

@@ -107,6 +107,31 @@ def test_layered_dup_blocks_parity(gpu, oracle, idx):
         assert_same_decode(r, ocode.decode(llr, 20, algo=oalgo, sched=1, msg16=True), code.k())
 
 
+@pytest.mark.parametrize("idx,sched,msg16,ebn0", [(6, 1, True, 1.1), (1, 1, True, 1.2), (6, 0, False, 1.1)])
+def test_spa_fast_against_fp64(gpu, oracle, idx, sched, msg16, ebn0):
+    """SFU sum-product: not bit-exact; judged against the FP64 sum-product oracle
+    (same schedule) by frame errors and by the deviation of the posteriors."""
+    code = dvb(idx)
+    ocode = oracle.Code.dvbt2(idx // 6, idx % 6)
+    info, _, llr = ocode.channel(21, 0, 48, ebn0)
+    dec = g.LdpcDecoder(code, algorithm=g.ALGO_SPA_FAST, schedule=sched,
+                        msg_dtype=g.MSG_F16 if msg16 else g.MSG_F32)
+    r = dec.decode_arrays(llr, 50, beliefs=True)
+    ref = ocode.decode_spa64(llr, 50, sched=sched)
+    bits = unpack_msg(r, code.k())
+    fe_gpu = int((bits != info).any(axis=1).sum())
+    fe_ref = int((ref["msg"] != info).any(axis=1).sum())
+    assert abs(fe_gpu - fe_ref) <= 2, (fe_gpu, fe_ref)
+    both = r["conv"] & ref["conv"]
+    assert both.sum() >= 0.8 * ref["conv"].sum()
+    assert (bits[both] == ref["msg"][both]).all()
+    # same decisions after one iteration, posteriors within 1e-2 relative + FP16 step
+    r1 = dec.decode_arrays(llr[:8], 1, beliefs=True)
+    ref1 = ocode.decode_spa64(llr[:8], 1, sched=sched)
+    dev = np.abs(r1["beliefs"] - ref1["beliefs"])
+    assert (dev <= 2e-2 * np.abs(ref1["beliefs"]) + 2e-2).mean() > 0.999
+
+
 @pytest.mark.parametrize("sched", [0, 1])
 def test_nms_parity(gpu, oracle, sched):
     code = g.LdpcCode.dvb_t2_short(g.CodeRate.Rate3_5)
