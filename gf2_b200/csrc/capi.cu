@@ -561,3 +561,94 @@ int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_of
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// learned normalised / offset min-sum trainer
+// ---------------------------------------------------------------------------
+struct gf2c_nms_trainer {
+  const gf2c_code* code = nullptr;
+  int T = 0, L = 1;
+  int64_t max_frames = 0;
+  int grid = 0;
+  long long work_stride = 0;
+  DevBuf dcode, X, B, work, sc_loss;
+};
+
+extern "C" {
+
+int gf2c_nms_trainer_create(const gf2c_code* code, int32_t iterations, int64_t max_frames, gf2c_nms_trainer** out) {
+  if (!code || !out || iterations <= 0 || iterations > 64 || max_frames <= 0)
+    return set_error(GF2C_ERR_INVALID_ARG, "bad arguments");
+  *out = nullptr;
+  const HostCode& h = *code->h;
+  if (h.max_dc > 32) return set_error(GF2C_ERR_UNSUPPORTED, "learned decoder: check degree above 32");
+  std::unique_ptr<gf2c_nms_trainer> tr(new (std::nothrow) gf2c_nms_trainer());
+  if (!tr) return set_error(GF2C_ERR_NOMEM, "out of host memory");
+  tr->code = code;
+  tr->T = iterations;
+  tr->L = h.layered_ok ? (int)h.cg.size() : 1;
+  tr->max_frames = max_frames;
+  int rc = code_dev_struct(code, tr->dcode);
+  if (rc) return rc;
+  const size_t E = (size_t)h.e_slots;
+  if ((rc = tr->X.ensure(sizeof(float) * E * iterations * (size_t)max_frames))) return rc;
+  if ((rc = tr->B.ensure(sizeof(float) * (size_t)h.n * (size_t)max_frames))) return rc;
+  int dev = 0, sms = 148;
+  GF2C_CUDA(cudaGetDevice(&dev));
+  GF2C_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  tr->grid = (int)std::min<int64_t>(max_frames, (int64_t)sms * 4);
+  tr->work_stride = (long long)(((E + 63) & ~(size_t)63) + (size_t)h.n + 64) * 4;
+  if ((rc = tr->work.ensure((size_t)tr->work_stride * tr->grid))) return rc;
+  *out = tr.release();
+  return GF2C_OK;
+}
+
+int gf2c_nms_trainer_destroy(gf2c_nms_trainer* tr) {
+  delete tr;
+  return GF2C_OK;
+}
+
+int gf2c_nms_trainer_layers(const gf2c_nms_trainer* tr, int32_t* layers) {
+  if (!tr || !layers) return set_error(GF2C_ERR_INVALID_ARG, "NULL argument");
+  *layers = tr->L;
+  return GF2C_OK;
+}
+
+int gf2c_nms_loss_grad(gf2c_nms_trainer* tr, const float* llr, const uint64_t* cw_bits, int64_t frames,
+                       const float* alpha, const float* beta, float* grad_alpha, float* grad_beta, float* loss,
+                       float* soft_out, void* stream) {
+  if (!tr || frames <= 0 || frames > tr->max_frames || !llr || !cw_bits || !alpha || !beta || !grad_alpha ||
+      !grad_beta || !loss)
+    return set_error(GF2C_ERR_INVALID_ARG, "bad arguments (frames must be in [1, max_frames])");
+  cudaStream_t st = (cudaStream_t)stream;
+  const DevCode& h = tr->code->h->dev;
+  const size_t nw = (size_t)tr->T * tr->L * sizeof(float);
+  GF2C_CUDA(cudaMemsetAsync(grad_alpha, 0, nw, st));
+  GF2C_CUDA(cudaMemsetAsync(grad_beta, 0, nw, st));
+  GF2C_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), st));
+  const int grid = (int)std::min<int64_t>(tr->grid, frames);
+  float* B = soft_out ? soft_out : (float*)tr->B.p;
+  int rc = launch_nms_forward((const DevCode*)tr->dcode.p, h, tr->T, tr->L, llr, cw_bits, frames, alpha, beta,
+                              (float*)tr->X.p, B, (char*)tr->work.p, tr->work_stride, grid, loss, st);
+  if (rc) return rc;
+  return launch_nms_backward((const DevCode*)tr->dcode.p, h, tr->T, tr->L, llr, cw_bits, frames, alpha, beta,
+                             (const float*)tr->X.p, B, (char*)tr->work.p, tr->work_stride, grid, grad_alpha,
+                             grad_beta, st);
+}
+
+int gf2c_count_errors(const uint64_t* ref_bits, const uint64_t* test_bits, int64_t frames, int32_t words,
+                      int32_t* bit_errors, uint64_t* totals, void* stream) {
+  if (frames < 0 || words <= 0 || (frames > 0 && (!ref_bits || !test_bits || !totals)))
+    return set_error(GF2C_ERR_INVALID_ARG, "bad arguments");
+  return launch_count_errors(ref_bits, test_bits, frames, words, bit_errors, (unsigned long long*)totals,
+                             (cudaStream_t)stream);
+}
+
+int gf2c_adam_step(float* params, const float* grads, float* m, float* v, int64_t count, float lr, float beta1,
+                   float beta2, float eps, int32_t step, float lo, float hi, void* stream) {
+  if (!params || !grads || !m || !v || count <= 0 || count > (1 << 30) || step < 1 || !(lo <= hi))
+    return set_error(GF2C_ERR_INVALID_ARG, "bad arguments");
+  return launch_adam(params, grads, m, v, (int)count, lr, beta1, beta2, eps, step, lo, hi, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -266,6 +266,50 @@ __global__ void __launch_bounds__(kEncThreads) channel_kernel(const DevCode* __r
   }
 }
 
+// Bit and frame errors between two packed bit batches (the FER / BER counters
+// of a Monte Carlo point; the reference's counterpart is the uncoded runner
+// SimulationRunner, crates/gf2-coding/src/simulation.rs:140-193).
+// totals[0] += frames with at least one error, totals[1] += bit errors.
+__global__ void __launch_bounds__(256) count_errors_kernel(const uint64_t* __restrict__ a,
+                                                           const uint64_t* __restrict__ b, long long frames,
+                                                           int words, int32_t* __restrict__ per_frame,
+                                                           unsigned long long* __restrict__ totals) {
+  __shared__ unsigned long long s_bits, s_frames;
+  if (threadIdx.x == 0) {
+    s_bits = 0;
+    s_frames = 0;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  for (long long f = (long long)blockIdx.x * nwarp + warp; f < frames; f += (long long)gridDim.x * nwarp) {
+    int e = 0;
+    for (int w = lane; w < words; w += 32) e += __popcll(a[f * words + w] ^ b[f * words + w]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if (lane == 0) {
+      if (per_frame) per_frame[f] = e;
+      if (e) {
+        atomicAdd(&s_bits, (unsigned long long)e);
+        atomicAdd(&s_frames, 1ull);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_frames) atomicAdd(&totals[0], s_frames);
+    if (s_bits) atomicAdd(&totals[1], s_bits);
+  }
+}
+
+int launch_count_errors(const uint64_t* a, const uint64_t* b, long long frames, int words, int32_t* per_frame,
+                        unsigned long long* totals, cudaStream_t st) {
+  if (frames <= 0) return GF2C_OK;
+  int grid = (int)std::min<long long>((frames + 7) / 8, 148 * 8);
+  count_errors_kernel<<<grid, 256, 0, st>>>(a, b, frames, words, per_frame, totals);
+  GF2C_CUDA(cudaGetLastError());
+  return GF2C_OK;
+}
+
 static int grid_for(long long frames) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);

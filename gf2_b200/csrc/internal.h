@@ -167,6 +167,17 @@ const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt);
 size_t layered_smem_bytes(int smem_app_floats, int bitmap_words, int parity_words);
 size_t decode_smem_bytes(int smem_app_floats, int bitmap_words);
 
+int launch_nms_forward(const DevCode* dcode, const DevCode& h, int T, int L, const float* llr, const uint64_t* cw,
+                       long long frames, const float* alpha, const float* beta, float* X, float* B, char* work,
+                       long long work_stride, int grid, float* loss, cudaStream_t st);
+int launch_nms_backward(const DevCode* dcode, const DevCode& h, int T, int L, const float* llr, const uint64_t* cw,
+                        long long frames, const float* alpha, const float* beta, const float* X, const float* B,
+                        char* work, long long work_stride, int grid, float* ga, float* gb, cudaStream_t st);
+int launch_count_errors(const uint64_t* a, const uint64_t* b, long long frames, int words, int32_t* per_frame,
+                        unsigned long long* totals, cudaStream_t st);
+int launch_adam(float* p, const float* g, float* m1, float* m2, int count, float lr, float b1, float b2, float eps,
+                int step, float lo, float hi, cudaStream_t st);
+
 int launch_syndrome(const DevCode* dcode, const DevCode& hcode, const uint64_t* cw, long long frames,
                     uint64_t* synd, int32_t* weight, cudaStream_t st);
 int launch_encode(const DevCode* dcode, const DevCode& hcode, const uint64_t* msg, long long frames,

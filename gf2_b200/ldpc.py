@@ -47,6 +47,12 @@ def unpack_bits(packed, nbits):
     return u[:, :nbits]
 
 
+# Bound at import time: object finalisers may run after module globals are
+# cleared at interpreter exit.
+_CODE_DESTROY = C.lib.gf2c_code_destroy
+_DECODER_DESTROY = C.lib.gf2c_decoder_destroy
+
+
 def _ptr(a):
     if a is None:
         return None
@@ -254,7 +260,7 @@ class LdpcCode:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            C.lib.gf2c_code_destroy(h)
+            _CODE_DESTROY(h)
             self._h = None
 
     @classmethod
@@ -410,7 +416,7 @@ class LdpcDecoder:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            C.lib.gf2c_decoder_destroy(h)
+            _DECODER_DESTROY(h)
             self._h = None
 
     def k(self):

@@ -185,6 +185,38 @@ int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_of
 /* Number of kernel launches issued by the last decode call of `dec`. */
 int gf2c_decoder_last_launches(const gf2c_decoder* dec, int32_t* launches);
 
+/* ---- learned normalised / offset min-sum (no reference counterpart: the
+ * reference only offers the fixed-weight rules Llr::boxplus_normalized_minsum_n
+ * and boxplus_offset_minsum_n, llr.rs:352-399) ----
+ * c2v = sign * alpha[t][l] * max(min|v2c| - beta[t][l], 0) for unrolled flooding
+ * iteration t < iterations and row group l < layers (layers = 1 for codes
+ * without row groups).  The trained weights decode with GF2C_ALGO_NMS. */
+typedef struct gf2c_nms_trainer gf2c_nms_trainer;
+int gf2c_nms_trainer_create(const gf2c_code* code, int32_t iterations, int64_t max_frames,
+                            gf2c_nms_trainer** out);
+int gf2c_nms_trainer_destroy(gf2c_nms_trainer* tr);
+int gf2c_nms_trainer_layers(const gf2c_nms_trainer* tr, int32_t* layers);
+/* Forward (iterations flooding steps, no early stop) and backward over a device
+ * batch: llr [frames][n] f32, cw_bits [frames][ceil(n/64)] transmitted codewords,
+ * alpha / beta [iterations][layers].  Writes the mean binary cross-entropy of
+ * sigmoid(final LLR) against the codeword bits to *loss and its gradients to
+ * grad_alpha / grad_beta (overwritten); soft_out [frames][n] (nullable) receives
+ * the final LLRs.  All pointers are device memory; asynchronous on `stream`. */
+int gf2c_nms_loss_grad(gf2c_nms_trainer* tr, const float* llr, const uint64_t* cw_bits, int64_t frames,
+                       const float* alpha, const float* beta, float* grad_alpha, float* grad_beta,
+                       float* loss, float* soft_out, void* stream);
+/* Frame / bit error counters of a Monte Carlo point (device memory): compares
+ * two packed batches of `words` words per frame; totals[0] += frames with an
+ * error, totals[1] += bit errors; bit_errors (nullable) receives the per-frame
+ * counts.  The reference only has an uncoded BER runner (SimulationRunner,
+ * simulation.rs:140-193); its coded FER loop lives in examples/ldpc_awgn.rs:121-175. */
+int gf2c_count_errors(const uint64_t* ref_bits, const uint64_t* test_bits, int64_t frames, int32_t words,
+                      int32_t* bit_errors, uint64_t* totals, void* stream);
+/* One Adam step (bias-corrected, step >= 1) on device arrays of `count` floats;
+ * parameters are clamped to [lo, hi]. */
+int gf2c_adam_step(float* params, const float* grads, float* m, float* v, int64_t count, float lr,
+                   float beta1, float beta2, float eps, int32_t step, float lo, float hi, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
