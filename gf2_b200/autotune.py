@@ -1,0 +1,89 @@
+"""Launch-shape autotuner for the decoders.
+
+A decoder runs a persistent kernel in which each CTA decodes one frame at a
+time; its launch shape is (threads per block, CTAs per SM), i.e. the check /
+variable tile a thread steps over and the number of frames in flight per SM.
+The autotuner times every feasible shape on a sample batch with CUDA events
+and keeps the fastest; results are cached in a JSON file keyed by device name,
+codes, algorithm, schedule and message type (GF2C_AUTOTUNE_CACHE overrides the
+default ~/.cache/gf2_b200/autotune.json).
+"""
+import json
+import os
+
+from .ldpc import LdpcDecoder
+
+
+def cache_path():
+    return os.environ.get("GF2C_AUTOTUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "gf2_b200", "autotune.json"))
+
+
+def _load():
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(d):
+    p = cache_path()
+    os.makedirs(os.path.dirname(p), exist_ok=True)
+    tmp = p + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
+    os.replace(tmp, p)
+
+
+def _key(codes, algorithm, schedule, msg_dtype, device_name):
+    cs = ",".join(f"{c.n()}x{c.m()}x{c.nnz()}" for c in codes)
+    return f"{device_name}|{cs}|a{algorithm}|s{schedule}|m{msg_dtype}"
+
+
+def candidates(codes, schedule):
+    """(threads per block, CTAs per SM) pairs; 0 = library choice.  The layered
+    schedule needs one thread per check of a row group, so only the number of
+    frames in flight per SM varies."""
+    if schedule == 1:
+        return [(0, b) for b in (1, 2, 3, 4)]
+    return [(t, b) for t in (128, 256, 384, 512) for b in (0, 1, 2, 3, 4)]
+
+
+def tune(codes, algorithm, schedule, msg_dtype, run, reps=3, nms_alpha=None, nms_beta=None, force=False):
+    """Return ((threads, blocks_per_sm), table).  `run(decoder)` decodes the
+    sample batch once on the current stream."""
+    import torch
+    dev_name = torch.cuda.get_device_name()
+    key = _key(codes, algorithm, schedule, msg_dtype, dev_name)
+    cache = _load()
+    if key in cache and not force:
+        e = cache[key]
+        return (e["threads"], e["blocks_per_sm"]), e.get("table", [])
+    table = []
+    best = None
+    for threads, bps in candidates(codes, schedule):
+        try:
+            dec = LdpcDecoder(codes[0], codes=codes, algorithm=algorithm, schedule=schedule, msg_dtype=msg_dtype,
+                              nms_alpha=nms_alpha, nms_beta=nms_beta, threads_per_block=threads,
+                              blocks_per_sm=bps)
+        except Exception:
+            continue
+        run(dec)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(reps):
+            run(dec)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / reps
+        table.append([threads, bps, ms])
+        if best is None or ms < best[2]:
+            best = (threads, bps, ms)
+        del dec
+    if best is None:
+        raise RuntimeError("no feasible launch shape")
+    cache[key] = {"threads": best[0], "blocks_per_sm": best[1], "ms": best[2], "table": table}
+    _store(cache)
+    return (best[0], best[1]), table
