@@ -8,6 +8,7 @@
 //   build_dvb_edges: (x + j q) mod m, staircase p / p-1       ldpc/dvb_t2/builder.rs:74-118
 //   QuasiCyclicLdpc::to_edges: row i -> col (i + s) mod Z     ldpc/core.rs:436-447, 578-605
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include "dvbt2_tables.h"
@@ -44,6 +45,11 @@ static void finish_sparse(HostCode& c, std::vector<std::vector<int64_t>>& per_ro
       next[v]++;
     }
   c.k = c.n > c.m ? c.n - c.m : 0;
+}
+
+uint64_t next_code_serial() {
+  static std::atomic<uint64_t> counter{0};
+  return ++counter;
 }
 
 static uint32_t pack_desc(int type, int base, int shift_or_q) {

@@ -58,8 +58,11 @@ struct DevCode {
   const int* enc_par_cols;         // kind 1: m parity columns
 };
 
+uint64_t next_code_serial();
+
 // Host-side code (reference-exact sparse structure + device layout plan).
 struct HostCode {
+  uint64_t serial = next_code_serial();    // unique per code object in the process
   int64_t n = 0, m = 0, k = 0;
   std::vector<int64_t> row_ptr, row_idx;   // CSR, columns ascending (sparse.rs:166-203)
   std::vector<int64_t> col_ptr, col_idx;   // CSC, rows ascending (sparse.rs:297-328)

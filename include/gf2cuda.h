@@ -182,6 +182,23 @@ int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_of
                       uint8_t* converged, uint8_t* syndrome_ok, int32_t use_graph,
                       int32_t mem, void* stream);
 
+/* Decoding without any device allocation -- no counterpart in the reference (its
+ * decoder is host code).  For callers that cannot call cudaMalloc: work being
+ * captured into a CUDA graph, processes whose device memory belongs to a pool or
+ * budget the library must not grow, real-time paths that forbid the allocator.
+ * Decodes `frames` frames of `code` exactly like gf2c_decode_batch with the
+ * default options (reference min-sum, flooding, f32, early stop); all pointers
+ * are device memory, asynchronous on `stream`.  Its scratch (the code's tables,
+ * the frame counter and the per-CTA workspace) is a 64 MiB static device array
+ * that every GPU loading the library holds until exit; codes whose tables plus
+ * one frame's workspace exceed it are rejected with GF2C_ERR_UNSUPPORTED.  The
+ * first call on a device looks up the array's device address and should come
+ * before any stream capture.  All calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller. */
+int gf2c_decode_batch_noalloc(const gf2c_code* code, const float* llr, int64_t frames, int32_t max_iter,
+                              uint64_t* msg_bits, int32_t* iterations, uint8_t* converged,
+                              uint8_t* syndrome_ok, void* stream);
+
 /* Number of kernel launches issued by the last decode call of `dec`. */
 int gf2c_decoder_last_launches(const gf2c_decoder* dec, int32_t* launches);
 
