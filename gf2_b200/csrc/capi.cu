@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <tuple>
@@ -61,6 +62,7 @@ struct gf2c_decoder {
   int max_n = 0, max_m = 0, max_words_k = 0, max_e_slots = 0, max_dc = 0, max_nchk = 0;
   int dcmax = 0, threads = 0, grid = 0, bitmap_words = 0, parity_words = 0, smem_app_floats = 0;
   const void* kernel = nullptr;
+  bool smem_flood = false;  // shared-memory-resident flooding min-sum kernel
   size_t smem = 0;
   long long work_stride = 0, app_offset = 0;
   DevBuf work, queue, status, alpha, beta;
@@ -355,8 +357,21 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   d->work_stride = c2v_bytes + (need_gapp ? ((long long)d->max_n * 4 + 255) / 256 * 256 : 0);
   d->kernel = layered ? layered_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax, threads)
                       : flood_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax);
+  // Flooding min-sum whose whole frame state (compressed check states and
+  // posteriors) fits in shared memory: the shared-memory-resident kernel.
+  const bool ms_family = o.algorithm == GF2C_ALGO_MINSUM || o.algorithm == GF2C_ALGO_NMS;
+  const size_t sf_bytes = smem_flood_bytes(d->max_n, d->max_m);
+  if (!layered && ms_family && d->max_dc <= 32 && sf_bytes <= (size_t)(224 * 1024) && !std::getenv("GF2C_NO_SMEM_FLOOD") &&
+      (o.threads_per_block == 0 || o.threads_per_block == 1024)) {
+    d->kernel = smem_flood_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax);
+    threads = 1024;
+    d->threads = threads;
+    d->smem = sf_bytes;
+    d->work_stride = 0;
+    d->smem_flood = true;
+  }
   if (!d->kernel) return set_error(GF2C_ERR_UNSUPPORTED, "no decode kernel for this configuration");
-  if (!layered && threads > 512)
+  if (!layered && !d->smem_flood && threads > 512)
     return set_error(GF2C_ERR_INVALID_ARG, "flooding schedule: threads_per_block must be <= 512");
   GF2C_CUDA(cudaFuncSetAttribute(d->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d->smem));
   int occ = 0;

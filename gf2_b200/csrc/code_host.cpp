@@ -103,11 +103,15 @@ static bool finish_plan(HostCode& c) {
   c.vg.assign(nvg, int2{0, 0});
   c.vg_slot.clear();
   c.vg_chk.clear();
-  std::vector<int> slot_cc(c.e_slots, -1);
+  c.vg_ci.clear();
+  std::vector<int> slot_cc(c.e_slots, -1), slot_i(c.e_slots, -1);
   for (size_t g = 0; g < c.cg.size(); g++) {
     int4 G = c.cg[g];
     for (int i = 0; i < G.z; i++)
-      for (int t = 0; t < G.y; t++) slot_cc[(size_t)G.w + (size_t)i * G.y + t] = G.x + t;
+      for (int t = 0; t < G.y; t++) {
+        slot_cc[(size_t)G.w + (size_t)i * G.y + t] = G.x + t;
+        slot_i[(size_t)G.w + (size_t)i * G.y + t] = i;
+      }
   }
   c.max_dv = 0;
   for (int h = 0; h < nvg; h++) {
@@ -121,6 +125,7 @@ static bool finish_plan(HostCode& c) {
     size_t base = c.vg_slot.size();
     c.vg_slot.resize(base + (size_t)dv * c.vgs, -1);
     c.vg_chk.resize(base + (size_t)dv * c.vgs, -1);
+    c.vg_ci.resize(base + (size_t)dv * c.vgs, -1);
     for (int j = 0; j < c.vgs; j++) {
       int64_t v = (int64_t)h * c.vgs + j;
       if (v >= c.n) break;
@@ -129,6 +134,7 @@ static bool finish_plan(HostCode& c) {
         const int sl = edge_slot[c.col_edge[s]];
         c.vg_slot[base + (size_t)i * c.vgs + j] = sl;
         c.vg_chk[base + (size_t)i * c.vgs + j] = slot_cc[sl];
+        c.vg_ci[base + (size_t)i * c.vgs + j] = slot_cc[sl] | (slot_i[sl] << 24);
       }
     }
     c.max_dv = std::max(c.max_dv, dv);
@@ -445,6 +451,7 @@ int upload_code(HostCode& c) {
     if ((rc = dev_copy(c, c.vg, &d.vg))) return rc;
     if ((rc = dev_copy(c, c.vg_slot, &d.vg_slot))) return rc;
     if ((rc = dev_copy(c, c.vg_chk, &d.vg_chk))) return rc;
+    if ((rc = dev_copy(c, c.vg_ci, &d.vg_ci))) return rc;
     if ((rc = dev_copy(c, c.slot_desc, &d.slot_desc))) return rc;
     if ((rc = dev_copy(c, c.slot_desc.empty() ? std::vector<int>() : c.cg_ninfo, &d.cg_ninfo))) return rc;
     d.z = c.slot_desc.empty() ? 0 : c.z;

@@ -41,6 +41,7 @@ struct DevCode {
   const int2* vg;                  // {dv, vedge0}
   const int* vg_slot;              // VG-major, [vg][i][j]
   const int* vg_chk;               // same layout: flattened check index of the edge
+  const int* vg_ci;                // same layout: flattened check | slot << 24
   // QC / DVB-T2 codes: slot i of check group g is described by slot_desc[edge0/Z + i]
   // (all Z checks of a row group share it), packed as base | shift_or_q << 20 | type << 30:
   //   type 0 circulant:   var = base + (t + shift) mod Z
@@ -81,6 +82,7 @@ struct HostCode {
   std::vector<int2> vg;
   std::vector<int> vg_slot;
   std::vector<int> vg_chk;
+  std::vector<int> vg_ci;
   std::vector<uint32_t> slot_desc;         // QC / DVB-T2 slot descriptors (see DevCode)
   std::vector<int> cg_ninfo;               // circulant slots per CG
   int vgs = 0, max_dc = 0, max_dv = 0, e_slots = 0, layered_ok = 0, max_nchk = 0;
@@ -164,6 +166,8 @@ struct DecodeArgs {
 };
 
 const void* flood_kernel_ptr(int algo, int msg16, int dcmax);
+const void* smem_flood_kernel_ptr(int algo, int msg16, int dcmax);
+size_t smem_flood_bytes(int n, int m);
 int decode_dcmax_bucket(int max_dc);
 int layered_dcmax_bucket(int max_dc);
 const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt);
