@@ -136,14 +136,16 @@ class ClockSampler:
 
 
 def read_traffic(workload):
-    """DRAM bytes per launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", f"bp_decode_{workload}.md")
-    try:
-        for line in open(path):
-            if line.strip().startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].split()[0])
-    except OSError:
-        pass
+    """DRAM bytes per launch from the committed ncu summary of the workload
+    (profiles/<kernel>_<workload>.md), if present."""
+    import glob
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", f"*_{workload}.md"))):
+        try:
+            for line in open(path):
+                if line.strip().startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+        except OSError:
+            pass
     return None
 
 
