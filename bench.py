@@ -12,6 +12,8 @@ Workloads (one "step" = one decode of the whole batch):
                 max 50 iterations with syndrome early stop; frame f at
                 Eb/N0 = 0.6 + 0.1 (f mod 9) dB (the 0.6..1.4 dB sweep in one batch).
   c2exact       c2 with the bit-exact FP32 sum-product numerics.
+  c2ref         the c2 frames with the reference's decoder (flooding min-sum
+                FP32, results bit-identical to the reference).
   c1            DVB-T2 short 1/2 (n=16200, k=7200), 256 frames, Eb/N0 1.0 dB,
                 flooding sum-product FP32 (bit-exact numerics), max 50 it.
   c1ref         the c1 frames with the reference's decoder (flooding min-sum FP32).
@@ -55,6 +57,10 @@ SINGLE = {
                     ebn0=[0.6 + 0.1 * i for i in range(9)],
                     desc="dvbt2-normal-3/5 layered sum-product (bit-exact numerics), fp16 messages, "
                          "4096 frames, Eb/N0 0.6..1.4 dB, max 50 it, early stop"),
+    "c2ref": dict(frame=0, rate=1, frames=4096, algo=0, sched=0, msg16=False, max_iter=50,
+                  ebn0=[0.6 + 0.1 * i for i in range(9)],
+                  desc="dvbt2-normal-3/5 flooding min-sum fp32 (reference decoder), 4096 frames, "
+                       "Eb/N0 0.6..1.4 dB (frame f at 0.6+0.1*(f mod 9)), max 50 it, early stop"),
     "c1": dict(frame=1, rate=0, frames=256, algo=1, sched=0, msg16=False, max_iter=50, ebn0=[1.0],
                desc="dvbt2-short-1/2 flooding sum-product fp32, 256 frames, Eb/N0 1.0 dB, max 50 it"),
     "c1ref": dict(frame=1, rate=0, frames=256, algo=0, sched=0, msg16=False, max_iter=50, ebn0=[1.0],
