@@ -62,7 +62,9 @@ struct gf2c_decoder {
   int max_n = 0, max_m = 0, max_words_k = 0, max_e_slots = 0, max_dc = 0, max_nchk = 0;
   int dcmax = 0, threads = 0, grid = 0, bitmap_words = 0, parity_words = 0, smem_app_floats = 0;
   const void* kernel = nullptr;
-  bool smem_flood = false;  // shared-memory-resident flooding min-sum kernel
+  bool state_flood = false;  // check-state flooding min-sum kernel (state_flood.cu)
+  int sf_st_smem = 0, sf_app_smem = 0;
+  long long sf_llr_off = 0, sf_st_off = 0, sf_app_off = 0;
   size_t smem = 0;
   long long work_stride = 0, app_offset = 0;
   DevBuf work, queue, status, alpha, beta;
@@ -357,21 +359,37 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   d->work_stride = c2v_bytes + (need_gapp ? ((long long)d->max_n * 4 + 255) / 256 * 256 : 0);
   d->kernel = layered ? layered_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax, threads)
                       : flood_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax);
-  // Flooding min-sum whose whole frame state (compressed check states and
-  // posteriors) fits in shared memory: the shared-memory-resident kernel.
+  // Flooding min-sum / normalised-offset min-sum: the check-state kernel, with
+  // the check states and posteriors in shared memory where they fit.
   const bool ms_family = o.algorithm == GF2C_ALGO_MINSUM || o.algorithm == GF2C_ALGO_NMS;
-  const size_t sf_bytes = smem_flood_bytes(d->max_n, d->max_m);
-  if (!layered && ms_family && d->max_dc <= 32 && sf_bytes <= (size_t)(224 * 1024) && !std::getenv("GF2C_NO_SMEM_FLOOD") &&
+  const int sf_dc = state_dcmax_bucket(d->max_dc);
+  if (!layered && ms_family && sf_dc > 0 && !std::getenv("GF2C_NO_STATE_FLOOD") &&
       (o.threads_per_block == 0 || o.threads_per_block == 1024)) {
-    d->kernel = smem_flood_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax);
+    const size_t budget = 224 * 1024;
+    const size_t st_bytes = (size_t)d->max_m * 16, app_bytes = (size_t)d->max_n * 4;
+    bool any_perm = false;
+    for (auto* c : d->codes) any_perm = any_perm || !c->h->sp_u2v.empty();
+    d->sf_st_smem = st_bytes <= budget;
+    d->sf_app_smem = st_bytes + app_bytes <= budget || (!d->sf_st_smem && app_bytes <= budget);
+    const bool all_smem = d->sf_st_smem && d->sf_app_smem;
+    auto al = [](long long x) { return (x + 255) / 256 * 256; };
+    long long off = 0;
+    d->sf_llr_off = off;
+    off += any_perm ? al(app_bytes) : 0;
+    d->sf_st_off = off;
+    off += d->sf_st_smem ? 0 : al(st_bytes);
+    d->sf_app_off = off;
+    off += d->sf_app_smem ? 0 : al(app_bytes);
+    d->work_stride = off;
+    d->smem = (d->sf_st_smem ? st_bytes : 0) + (d->sf_app_smem ? app_bytes : 0);
+    d->kernel = state_flood_kernel_ptr(sf_dc, all_smem);
+    d->dcmax = sf_dc;
     threads = 1024;
     d->threads = threads;
-    d->smem = sf_bytes;
-    d->work_stride = 0;
-    d->smem_flood = true;
+    d->state_flood = true;
   }
   if (!d->kernel) return set_error(GF2C_ERR_UNSUPPORTED, "no decode kernel for this configuration");
-  if (!layered && !d->smem_flood && threads > 512)
+  if (!layered && !d->state_flood && threads > 512)
     return set_error(GF2C_ERR_INVALID_ARG, "flooding schedule: threads_per_block must be <= 512");
   GF2C_CUDA(cudaFuncSetAttribute(d->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d->smem));
   int occ = 0;
@@ -419,6 +437,12 @@ static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaSt
   a.nms_L = d->nms_L;
   a.early_stop = d->opts.early_stop;
   a.status = (int*)d->status.p;
+  a.sf_st_smem = d->sf_st_smem;
+  a.sf_app_smem = d->sf_app_smem;
+  a.sf_msg16 = d->opts.msg_dtype == GF2C_MSG_F16;
+  a.sf_llr_off = d->sf_llr_off;
+  a.sf_st_off = d->sf_st_off;
+  a.sf_app_off = d->sf_app_off;
   GF2C_CUDA(cudaMemsetAsync(d->queue.p, 0, sizeof(unsigned long long), st));
   int grid = (int)std::min<int64_t>(d->grid, frames);
   d->last_launches = 1;

@@ -142,6 +142,94 @@ static bool finish_plan(HostCode& c) {
   return true;
 }
 
+// Check-state flooding plan.  DVB-T2 parity bits are stored transposed (u order,
+// see DevCode); every other code keeps the natural order.  For codes with slot
+// descriptors each (CG, slot) is refitted in u order as base + (t + shift) mod Z
+// with an optional missing t = 0 (the staircase corner); if any slot does not
+// fit, the plan falls back to the natural order and the slot table.
+void plan_state(HostCode& c) {
+  const int64_t n = c.n;
+  std::vector<int> u_of(n), v_of(n);
+  for (int64_t v = 0; v < n; v++) u_of[v] = (int)v;
+  if (c.kind == 2) {
+    const int64_t k = c.k, q = c.q, Z = c.z;
+    for (int64_t p = 0; p < c.m; p++) u_of[k + p] = (int)(k + (p % q) * Z + p / q);
+  }
+  c.sp_desc.clear();
+  c.sp_cg.clear();
+  bool structured = !c.slot_desc.empty() && n < (1 << 20);
+  for (size_t g = 0; g < c.cg.size() && structured; g++) {
+    const int4 G = c.cg[g];
+    const int Z = G.y;
+    if (Z > 1023) structured = false;
+    for (int i = 0; i < G.z && structured; i++) {
+      std::vector<int> u(Z);
+      int base = INT32_MAX, t1 = -1;
+      for (int t = 0; t < Z; t++) {
+        const int v = c.slot_var[(size_t)G.w + (size_t)i * Z + t];
+        u[t] = v < 0 ? -1 : u_of[v];
+        if (u[t] >= 0) {
+          base = std::min(base, u[t]);
+          if (t1 < 0) t1 = t;
+        } else if (t > 0) {
+          structured = false;
+        }
+      }
+      if (!structured || t1 < 0) {
+        structured = false;
+        break;
+      }
+      const int sh = (int)((((int64_t)u[t1] - base - t1) % Z + Z) % Z);
+      for (int t = 0; t < Z && structured; t++)
+        if (u[t] >= 0 && u[t] != base + (t + sh) % Z) structured = false;
+      c.sp_desc.push_back((uint32_t)base | ((uint32_t)sh << 20) | ((u[0] < 0 ? 1u : 0u) << 31));
+    }
+  }
+  if (!structured) {
+    c.sp_desc.clear();
+    for (int64_t v = 0; v < n; v++) u_of[v] = (int)v;
+  }
+  bool identity = true;
+  for (int64_t v = 0; v < n; v++) {
+    v_of[u_of[v]] = (int)v;
+    identity = identity && u_of[v] == v;
+  }
+  c.sp_u2v.clear();
+  if (!identity) c.sp_u2v = v_of;
+  int desc_off = 0;
+  c.sp_cchunk.clear();
+  for (size_t g = 0; g < c.cg.size(); g++) {
+    const int4 G = c.cg[g];
+    c.sp_cg.push_back(int4{G.x, G.y, G.z, structured ? desc_off : G.w});
+    desc_off += G.z;
+    for (int t0 = 0; t0 < G.y; t0 += 32) c.sp_cchunk.push_back(int2{(int)g, t0});
+  }
+  // u-order var groups of vgs variables; edge lists copied from the natural ones
+  const int vgs = c.vgs;
+  const int nvg = (int)((n + vgs - 1) / vgs);
+  c.sp_vg.assign(nvg, int2{0, 0});
+  c.sp_ci.clear();
+  c.sp_vchunk.clear();
+  for (int h = 0; h < nvg; h++) {
+    int dv = 0;
+    for (int j = 0; j < vgs && (int64_t)h * vgs + j < n; j++) {
+      const int v = v_of[(size_t)h * vgs + j];
+      dv = std::max(dv, (int)(c.col_ptr[v + 1] - c.col_ptr[v]));
+    }
+    const size_t off = c.sp_ci.size();
+    c.sp_vg[h] = int2{dv, (int)off};
+    c.sp_ci.resize(off + (size_t)dv * vgs, -1);
+    for (int j = 0; j < vgs && (int64_t)h * vgs + j < n; j++) {
+      const int v = v_of[(size_t)h * vgs + j];
+      const int hv = v / vgs, jv = v - hv * vgs;
+      const int2 V = c.vg[hv];
+      const int deg = (int)(c.col_ptr[v + 1] - c.col_ptr[v]);
+      for (int i = 0; i < deg; i++) c.sp_ci[off + (size_t)i * vgs + j] = c.vg_ci[(size_t)V.y + (size_t)i * vgs + jv];
+    }
+    for (int j0 = 0; j0 < vgs && (int64_t)h * vgs + j0 < n; j0 += 32) c.sp_vchunk.push_back(int2{h, j0});
+  }
+}
+
 // Generic plan: CGs of up to 256 consecutive checks, slots in CSR order.
 static void plan_generic(HostCode& c) {
   c.cg.clear();
@@ -189,6 +277,7 @@ int build_edges(int64_t m, int64_t n, const int64_t* pairs, int64_t count, HostC
   finish_sparse(c, per_row);
   c.kind = 0;
   plan_generic(c);
+  plan_state(c);
   return GF2C_OK;
 }
 
@@ -244,6 +333,7 @@ int build_qc(const int32_t* base, int mb, int nb, int z, HostCode& c) {
     c.slot_desc.clear();
     plan_generic(c);
   }
+  plan_state(c);
   return GF2C_OK;
 }
 
@@ -334,6 +424,7 @@ int build_dvbt2(int frame, int rate, HostCode& c) {
       }
     }
   }
+  plan_state(c);
   return GF2C_OK;
 }
 
@@ -455,6 +546,15 @@ int upload_code(HostCode& c) {
     if ((rc = dev_copy(c, c.slot_desc, &d.slot_desc))) return rc;
     if ((rc = dev_copy(c, c.slot_desc.empty() ? std::vector<int>() : c.cg_ninfo, &d.cg_ninfo))) return rc;
     d.z = c.slot_desc.empty() ? 0 : c.z;
+    if ((rc = dev_copy(c, c.sp_cg, &d.sp_cg))) return rc;
+    if ((rc = dev_copy(c, c.sp_desc, &d.sp_desc))) return rc;
+    if ((rc = dev_copy(c, c.sp_cchunk, &d.sp_cchunk))) return rc;
+    if ((rc = dev_copy(c, c.sp_vg, &d.sp_vg))) return rc;
+    if ((rc = dev_copy(c, c.sp_ci, &d.sp_ci))) return rc;
+    if ((rc = dev_copy(c, c.sp_vchunk, &d.sp_vchunk))) return rc;
+    if ((rc = dev_copy(c, c.sp_u2v, &d.sp_u2v))) return rc;
+    d.sp_ncchunk = (int)c.sp_cchunk.size();
+    d.sp_nvchunk = (int)c.sp_vchunk.size();
     std::vector<int> rp(c.row_ptr.begin(), c.row_ptr.end()), ri(c.row_idx.begin(), c.row_idx.end());
     if ((rc = dev_copy(c, rp, &d.csr_ptr))) return rc;
     if ((rc = dev_copy(c, ri, &d.csr_idx))) return rc;

@@ -50,6 +50,21 @@ struct DevCode {
   const uint32_t* slot_desc;       // nullptr for codes without the QC structure
   const int* cg_ninfo;             // per CG: number of circulant slots (the rest are staircase)
   int z;                           // circulant size of slot_desc codes
+  // Check-state flooding kernel (state_flood.cu).  Variables are stored in a
+  // "u order": the identity, except for DVB-T2 codes whose parity bit
+  // k + a + q t is stored at k + a Z + t, which makes every slot of every row
+  // group a contiguous (rotated) run of Z posteriors.
+  const int4* sp_cg;               // per CG {chk_begin, nchk, dc, desc offset (structured) | edge0}
+  const uint32_t* sp_desc;         // u-order slot descriptors base | shift << 20 | absent_at_t0 << 31
+                                   // (nullptr: u order is the identity and slot_var is used)
+  const int2* sp_cchunk;           // check chunks {CG, first check in CG}: 32 checks of one CG
+  int sp_ncchunk;
+  const int2* sp_vg;               // per u-order var group of vgs variables {dv, offset into sp_ci}
+  const int* sp_ci;                // [offset + i * vgs + j]: flattened check | slot << 24 of edge i,
+                                   // ascending original check index; -1 = pad
+  const int2* sp_vchunk;           // var chunks {var group, first j}: 32 variables of one group
+  int sp_nvchunk;
+  const int* sp_u2v;               // natural index of u-order variable u (nullptr: identity)
   const int* csr_ptr;              // natural order H (m + 1)
   const int* csr_idx;              // (nnz)
   // encoder
@@ -87,6 +102,11 @@ struct HostCode {
   std::vector<int> cg_ninfo;               // circulant slots per CG
   int vgs = 0, max_dc = 0, max_dv = 0, e_slots = 0, layered_ok = 0, max_nchk = 0;
   std::vector<int64_t> cg_checks;          // original check of each flattened check
+  // check-state flooding plan (see DevCode)
+  std::vector<int4> sp_cg;
+  std::vector<uint32_t> sp_desc;
+  std::vector<int2> sp_cchunk, sp_vg, sp_vchunk;
+  std::vector<int> sp_ci, sp_u2v;
 
   // encoder (generic)
   int enc_kind = 0;
@@ -129,6 +149,7 @@ int cuda_error(cudaError_t e, const char* what);
 int build_dvbt2(int frame, int rate, HostCode& c);
 int build_qc(const int32_t* base, int mb, int nb, int z, HostCode& c);
 int build_edges(int64_t m, int64_t n, const int64_t* pairs, int64_t count, HostCode& c);
+void plan_state(HostCode& c);  // the check-state flooding plan (after the CG / VG plan)
 int prepare_encoder(HostCode& c);
 int upload_code(HostCode& c);  // uploads the device layout on the current device
 
@@ -163,11 +184,15 @@ struct DecodeArgs {
   int nms_L;
   int early_stop;
   int* status;                     // kernel-side error flag
+  // check-state flooding kernel: which arrays live in shared memory, and the
+  // offsets of the others in the CTA workspace (u-order LLRs always there)
+  int sf_st_smem, sf_app_smem, sf_msg16;
+  long long sf_llr_off, sf_st_off, sf_app_off;
 };
 
 const void* flood_kernel_ptr(int algo, int msg16, int dcmax);
-const void* smem_flood_kernel_ptr(int algo, int msg16, int dcmax);
-size_t smem_flood_bytes(int n, int m);
+int state_dcmax_bucket(int max_dc);
+const void* state_flood_kernel_ptr(int dcmax, bool all_smem);
 int decode_dcmax_bucket(int max_dc);
 int layered_dcmax_bucket(int max_dc);
 const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt);

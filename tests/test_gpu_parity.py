@@ -146,6 +146,40 @@ def test_nms_parity(gpu, oracle, sched):
     assert_same_decode(r, ocode.decode(llr, 20, algo=3, sched=sched, alpha=a, beta=b), code.k())
 
 
+@pytest.mark.parametrize("idx,msg16", [(6, True), (1, True), (3, False)])
+def test_minsum_flooding_fp16_and_placements(gpu, oracle, idx, msg16):
+    """Check-state kernel: FP16 magnitudes (short 1/2: states and posteriors in
+    shared memory; normal 3/5: both in the workspace) and normal 3/4 (states in
+    the workspace, 16200 checks)."""
+    code = dvb(idx)
+    ocode = oracle.Code.dvbt2(idx // 6, idx % 6)
+    _, _, llr = ocode.channel(12, 3, 10, 1.0 if idx != 3 else 2.6)
+    dec = g.LdpcDecoder(code, msg_dtype=g.MSG_F16 if msg16 else g.MSG_F32)
+    r = dec.decode_arrays(llr, 25, beliefs=True)
+    assert_same_decode(r, ocode.decode(llr, 25, msg16=msg16), code.k())
+
+
+def test_minsum_flooding_qc_and_normal_nms(gpu, oracle):
+    # a QC code (identity variable order, circulant descriptors)
+    rng = np.random.default_rng(5)
+    base = [[int(s) if rng.random() < 0.7 else -1 for s in rng.integers(0, 96, 24)] for _ in range(8)]
+    q = g.LdpcCode.from_quasi_cyclic(g.QuasiCyclicLdpc(base, 96))
+    oq = oracle.Code.qc(base, 96)
+    llr = rng.normal(1.2, 1.5, (12, q.n())).astype(np.float32)
+    r = g.LdpcDecoder(q).decode_arrays(llr, 15, beliefs=True)
+    assert_same_decode(r, oq.decode(llr, 15), q.k())
+    # normalised / offset min-sum on a normal frame (per-row-group weights)
+    code = dvb(2)
+    ocode = oracle.Code.dvbt2(0, 2)
+    _, _, llr = ocode.channel(13, 0, 6, 2.0)
+    T, L = 5, code.layers()
+    a = (0.6 + 0.4 * rng.random((T, L))).astype(np.float32)
+    b = (0.3 * rng.random((T, L))).astype(np.float32)
+    dec = g.LdpcDecoder(code, algorithm=g.ALGO_NMS, nms_alpha=a, nms_beta=b)
+    r = dec.decode_arrays(llr, 12, beliefs=True)
+    assert_same_decode(r, ocode.decode(llr, 12, algo=3, alpha=a, beta=b), code.k())
+
+
 def test_device_tensor_path_matches_host(gpu, oracle):
     import torch
     code = g.LdpcCode.dvb_t2_short(g.CodeRate.Rate2_3)
