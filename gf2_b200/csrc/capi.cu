@@ -63,7 +63,7 @@ struct gf2c_decoder {
   int dcmax = 0, threads = 0, grid = 0, bitmap_words = 0, parity_words = 0, smem_app_floats = 0;
   const void* kernel = nullptr;
   bool state_flood = false;  // check-state flooding min-sum kernel (state_flood.cu)
-  int sf_st_smem = 0, sf_app_smem = 0;
+  int sf_app_soff = 0;
   long long sf_llr_off = 0, sf_st_off = 0, sf_app_off = 0;
   size_t smem = 0;
   long long work_stride = 0, app_offset = 0;
@@ -364,27 +364,29 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   const bool ms_family = o.algorithm == GF2C_ALGO_MINSUM || o.algorithm == GF2C_ALGO_NMS;
   const int sf_dc = state_dcmax_bucket(d->max_dc);
   if (!layered && ms_family && sf_dc > 0 && !std::getenv("GF2C_NO_STATE_FLOOD") &&
-      (o.threads_per_block == 0 || o.threads_per_block == 1024)) {
+      (o.threads_per_block == 0 || o.threads_per_block == state_flood_threads())) {
     const size_t budget = 224 * 1024;
     const size_t st_bytes = (size_t)d->max_m * 16, app_bytes = (size_t)d->max_n * 4;
     bool any_perm = false;
     for (auto* c : d->codes) any_perm = any_perm || !c->h->sp_u2v.empty();
-    d->sf_st_smem = st_bytes <= budget;
-    d->sf_app_smem = st_bytes + app_bytes <= budget || (!d->sf_st_smem && app_bytes <= budget);
-    const bool all_smem = d->sf_st_smem && d->sf_app_smem;
+    // Either the whole frame state is on chip, or all of it is in the workspace:
+    // keeping only part of it in shared memory (measured on normal 3/5 frames)
+    // shrinks L1, which caches the workspace, by more than it saves in L2 traffic.
+    const bool all_smem = st_bytes + app_bytes <= budget;
+    d->sf_app_soff = (int)st_bytes;
     auto al = [](long long x) { return (x + 255) / 256 * 256; };
     long long off = 0;
     d->sf_llr_off = off;
     off += any_perm ? al(app_bytes) : 0;
     d->sf_st_off = off;
-    off += d->sf_st_smem ? 0 : al(st_bytes);
+    off += all_smem ? 0 : al(st_bytes);
     d->sf_app_off = off;
-    off += d->sf_app_smem ? 0 : al(app_bytes);
+    off += all_smem ? 0 : al(app_bytes);
     d->work_stride = off;
-    d->smem = (d->sf_st_smem ? st_bytes : 0) + (d->sf_app_smem ? app_bytes : 0);
+    d->smem = all_smem ? st_bytes + app_bytes : 0;
     d->kernel = state_flood_kernel_ptr(sf_dc, all_smem);
     d->dcmax = sf_dc;
-    threads = 1024;
+    threads = state_flood_threads();
     d->threads = threads;
     d->state_flood = true;
   }
@@ -437,8 +439,7 @@ static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaSt
   a.nms_L = d->nms_L;
   a.early_stop = d->opts.early_stop;
   a.status = (int*)d->status.p;
-  a.sf_st_smem = d->sf_st_smem;
-  a.sf_app_smem = d->sf_app_smem;
+  a.sf_app_soff = d->sf_app_soff;
   a.sf_msg16 = d->opts.msg_dtype == GF2C_MSG_F16;
   a.sf_llr_off = d->sf_llr_off;
   a.sf_st_off = d->sf_st_off;
@@ -610,7 +611,7 @@ struct gf2c_nms_trainer {
   int64_t max_frames = 0;
   int grid = 0;
   long long work_stride = 0;
-  DevBuf dcode, X, B, work, sc_loss;
+  DevBuf dcode, X, B, work, pf;  // pf: per-frame gradients and loss, [frames][2 T L + 1]
 };
 
 extern "C" {
@@ -636,8 +637,9 @@ int gf2c_nms_trainer_create(const gf2c_code* code, int32_t iterations, int64_t m
   GF2C_CUDA(cudaGetDevice(&dev));
   GF2C_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   tr->grid = (int)std::min<int64_t>(max_frames, (int64_t)sms * 4);
-  tr->work_stride = (long long)(((E + 63) & ~(size_t)63) + (size_t)h.n + 64) * 4;
+  tr->work_stride = (long long)(((E + 63) & ~(size_t)63) + (((size_t)h.n + 63) & ~(size_t)63) + 2 * (size_t)h.m + 64) * 4;
   if ((rc = tr->work.ensure((size_t)tr->work_stride * tr->grid))) return rc;
+  if ((rc = tr->pf.ensure(sizeof(float) * (size_t)max_frames * (2 * (size_t)iterations * tr->L + 1)))) return rc;
   *out = tr.release();
   return GF2C_OK;
 }
@@ -661,18 +663,14 @@ int gf2c_nms_loss_grad(gf2c_nms_trainer* tr, const float* llr, const uint64_t* c
     return set_error(GF2C_ERR_INVALID_ARG, "bad arguments (frames must be in [1, max_frames])");
   cudaStream_t st = (cudaStream_t)stream;
   const DevCode& h = tr->code->h->dev;
-  const size_t nw = (size_t)tr->T * tr->L * sizeof(float);
-  GF2C_CUDA(cudaMemsetAsync(grad_alpha, 0, nw, st));
-  GF2C_CUDA(cudaMemsetAsync(grad_beta, 0, nw, st));
-  GF2C_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), st));
   const int grid = (int)std::min<int64_t>(tr->grid, frames);
   float* B = soft_out ? soft_out : (float*)tr->B.p;
   int rc = launch_nms_forward((const DevCode*)tr->dcode.p, h, tr->T, tr->L, llr, cw_bits, frames, alpha, beta,
-                              (float*)tr->X.p, B, (char*)tr->work.p, tr->work_stride, grid, loss, st);
+                              (float*)tr->X.p, B, (char*)tr->work.p, tr->work_stride, grid, (float*)tr->pf.p, st);
   if (rc) return rc;
   return launch_nms_backward((const DevCode*)tr->dcode.p, h, tr->T, tr->L, llr, cw_bits, frames, alpha, beta,
-                             (const float*)tr->X.p, B, (char*)tr->work.p, tr->work_stride, grid, grad_alpha,
-                             grad_beta, st);
+                             (const float*)tr->X.p, B, (char*)tr->work.p, tr->work_stride, grid, (float*)tr->pf.p,
+                             grad_alpha, grad_beta, loss, st);
 }
 
 int gf2c_count_errors(const uint64_t* ref_bits, const uint64_t* test_bits, int64_t frames, int32_t words,

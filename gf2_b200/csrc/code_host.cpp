@@ -146,7 +146,9 @@ static bool finish_plan(HostCode& c) {
 // see DevCode); every other code keeps the natural order.  For codes with slot
 // descriptors each (CG, slot) is refitted in u order as base + (t + shift) mod Z
 // with an optional missing t = 0 (the staircase corner); if any slot does not
-// fit, the plan falls back to the natural order and the slot table.
+// fit, the plan falls back to the natural order and the slot table.  A slot
+// with shift s is stored as {start = base + s, wrap = Z - s}; the variable of a
+// missing t = 0 entry is start itself (a valid index, masked by sp_absent).
 void plan_state(HostCode& c) {
   const int64_t n = c.n;
   std::vector<int> u_of(n), v_of(n);
@@ -156,12 +158,14 @@ void plan_state(HostCode& c) {
     for (int64_t p = 0; p < c.m; p++) u_of[k + p] = (int)(k + (p % q) * Z + p / q);
   }
   c.sp_desc.clear();
+  c.sp_absent.clear();
   c.sp_cg.clear();
-  bool structured = !c.slot_desc.empty() && n < (1 << 20);
+  bool structured = !c.slot_desc.empty() && n < (1 << 30);
   for (size_t g = 0; g < c.cg.size() && structured; g++) {
     const int4 G = c.cg[g];
     const int Z = G.y;
-    if (Z > 1023) structured = false;
+    if (G.z > 32) structured = false;
+    uint32_t absent = 0;
     for (int i = 0; i < G.z && structured; i++) {
       std::vector<int> u(Z);
       int base = INT32_MAX, t1 = -1;
@@ -180,13 +184,17 @@ void plan_state(HostCode& c) {
         break;
       }
       const int sh = (int)((((int64_t)u[t1] - base - t1) % Z + Z) % Z);
+      if ((int64_t)base + Z > n) structured = false;  // every start + t must be a valid index
       for (int t = 0; t < Z && structured; t++)
         if (u[t] >= 0 && u[t] != base + (t + sh) % Z) structured = false;
-      c.sp_desc.push_back((uint32_t)base | ((uint32_t)sh << 20) | ((u[0] < 0 ? 1u : 0u) << 31));
+      c.sp_desc.push_back(int2{base + sh, Z - sh});
+      if (u[0] < 0) absent |= 1u << i;
     }
+    c.sp_absent.push_back(absent);
   }
   if (!structured) {
     c.sp_desc.clear();
+    c.sp_absent.clear();
     for (int64_t v = 0; v < n; v++) u_of[v] = (int)v;
   }
   bool identity = true;
@@ -207,7 +215,7 @@ void plan_state(HostCode& c) {
   // u-order var groups of vgs variables; edge lists copied from the natural ones
   const int vgs = c.vgs;
   const int nvg = (int)((n + vgs - 1) / vgs);
-  c.sp_vg.assign(nvg, int2{0, 0});
+  std::vector<int2> vg2(nvg, int2{0, 0});
   c.sp_ci.clear();
   c.sp_vchunk.clear();
   for (int h = 0; h < nvg; h++) {
@@ -217,7 +225,7 @@ void plan_state(HostCode& c) {
       dv = std::max(dv, (int)(c.col_ptr[v + 1] - c.col_ptr[v]));
     }
     const size_t off = c.sp_ci.size();
-    c.sp_vg[h] = int2{dv, (int)off};
+    vg2[h] = int2{dv, (int)off};
     c.sp_ci.resize(off + (size_t)dv * vgs, -1);
     for (int j = 0; j < vgs && (int64_t)h * vgs + j < n; j++) {
       const int v = v_of[(size_t)h * vgs + j];
@@ -228,6 +236,7 @@ void plan_state(HostCode& c) {
     }
     for (int j0 = 0; j0 < vgs && (int64_t)h * vgs + j0 < n; j0 += 32) c.sp_vchunk.push_back(int2{h, j0});
   }
+  c.sp_vg = vg2;
 }
 
 // Generic plan: CGs of up to 256 consecutive checks, slots in CSR order.
@@ -548,6 +557,7 @@ int upload_code(HostCode& c) {
     d.z = c.slot_desc.empty() ? 0 : c.z;
     if ((rc = dev_copy(c, c.sp_cg, &d.sp_cg))) return rc;
     if ((rc = dev_copy(c, c.sp_desc, &d.sp_desc))) return rc;
+    if ((rc = dev_copy(c, c.sp_absent, &d.sp_absent))) return rc;
     if ((rc = dev_copy(c, c.sp_cchunk, &d.sp_cchunk))) return rc;
     if ((rc = dev_copy(c, c.sp_vg, &d.sp_vg))) return rc;
     if ((rc = dev_copy(c, c.sp_ci, &d.sp_ci))) return rc;

@@ -55,8 +55,10 @@ struct DevCode {
   // k + a + q t is stored at k + a Z + t, which makes every slot of every row
   // group a contiguous (rotated) run of Z posteriors.
   const int4* sp_cg;               // per CG {chk_begin, nchk, dc, desc offset (structured) | edge0}
-  const uint32_t* sp_desc;         // u-order slot descriptors base | shift << 20 | absent_at_t0 << 31
-                                   // (nullptr: u order is the identity and slot_var is used)
+  const int2* sp_desc;             // u-order slot descriptors {start, wrap}: check t reads variable
+                                   // start + t - (t >= wrap ? nchk : 0) (nullptr: u order is the
+                                   // identity and slot_var is used)
+  const uint32_t* sp_absent;       // per CG: slots without an edge at check t = 0 (staircase corner)
   const int2* sp_cchunk;           // check chunks {CG, first check in CG}: 32 checks of one CG
   int sp_ncchunk;
   const int2* sp_vg;               // per u-order var group of vgs variables {dv, offset into sp_ci}
@@ -104,8 +106,9 @@ struct HostCode {
   std::vector<int64_t> cg_checks;          // original check of each flattened check
   // check-state flooding plan (see DevCode)
   std::vector<int4> sp_cg;
-  std::vector<uint32_t> sp_desc;
-  std::vector<int2> sp_cchunk, sp_vg, sp_vchunk;
+  std::vector<int2> sp_desc;
+  std::vector<uint32_t> sp_absent;
+  std::vector<int2> sp_cchunk, sp_vchunk, sp_vg;
   std::vector<int> sp_ci, sp_u2v;
 
   // encoder (generic)
@@ -184,14 +187,17 @@ struct DecodeArgs {
   int nms_L;
   int early_stop;
   int* status;                     // kernel-side error flag
-  // check-state flooding kernel: which arrays live in shared memory, and the
-  // offsets of the others in the CTA workspace (u-order LLRs always there)
-  int sf_st_smem, sf_app_smem, sf_msg16;
+  // check-state flooding kernel: byte offset of the posteriors in shared memory
+  // (frame state on chip) and the offsets in the CTA workspace of the u-order
+  // LLRs, the check states and the posteriors (frame state in the workspace)
+  int sf_msg16;
+  int sf_app_soff;
   long long sf_llr_off, sf_st_off, sf_app_off;
 };
 
 const void* flood_kernel_ptr(int algo, int msg16, int dcmax);
 int state_dcmax_bucket(int max_dc);
+int state_flood_threads();
 const void* state_flood_kernel_ptr(int dcmax, bool all_smem);
 int decode_dcmax_bucket(int max_dc);
 int layered_dcmax_bucket(int max_dc);
@@ -201,10 +207,11 @@ size_t decode_smem_bytes(int smem_app_floats, int bitmap_words);
 
 int launch_nms_forward(const DevCode* dcode, const DevCode& h, int T, int L, const float* llr, const uint64_t* cw,
                        long long frames, const float* alpha, const float* beta, float* X, float* B, char* work,
-                       long long work_stride, int grid, float* loss, cudaStream_t st);
+                       long long work_stride, int grid, float* pf, cudaStream_t st);
 int launch_nms_backward(const DevCode* dcode, const DevCode& h, int T, int L, const float* llr, const uint64_t* cw,
                         long long frames, const float* alpha, const float* beta, const float* X, const float* B,
-                        char* work, long long work_stride, int grid, float* ga, float* gb, cudaStream_t st);
+                        char* work, long long work_stride, int grid, float* pf, float* ga, float* gb,
+                        float* loss, cudaStream_t st);
 int launch_count_errors(const uint64_t* a, const uint64_t* b, long long frames, int words, int32_t* per_frame,
                         unsigned long long* totals, cudaStream_t st);
 int launch_adam(float* p, const float* g, float* m1, float* m2, int count, float lr, float b1, float b2, float eps,

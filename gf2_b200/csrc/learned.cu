@@ -14,9 +14,12 @@
 // nms_backward_kernel: one CTA per frame, t = T-1 .. 0.  The min routes the
 //   gradient to the first index attaining it among the other edges, so inside
 //   a check only the two smallest-magnitude slots receive gradient; d|x|/dx =
-//   -1 if x < 0 else +1; d max(u, 0)/du = [u > 0].  Weight gradients are
-//   summed per (t, row group) in shared memory and added to the global
-//   gradient with one atomic per CTA.
+//   -1 if x < 0 else +1; d max(u, 0)/du = [u > 0].
+// Reductions are deterministic (no floating-point atomics): each check
+// writes its weight-gradient terms to the CTA workspace, one warp per row
+// group sums them in a fixed order, each frame's gradients and loss go to its
+// own row of a per-frame buffer, and nms_reduce_kernel sums the frames in
+// order.  Training is therefore bit-reproducible.
 // adam_kernel: Adam (Kingma & Ba 2015) with bias correction.
 #include "internal.h"
 #include "numeric.cuh"
@@ -39,6 +42,13 @@ __device__ __forceinline__ LearnCtx make_ctx(const DevCode& C, int L) {
   return LearnCtx{C.n, C.m, C.ncg, C.vgs, L, C.cg, C.slot_var, C.chk_cg, C.vg, C.vg_slot};
 }
 
+// Sum over a warp in a fixed order (butterfly), every lane gets the total.
+__device__ __forceinline__ float warp_sum_fixed(float x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = __fadd_rn(x, __shfl_xor_sync(0xffffffffu, x, o));
+  return x;
+}
+
 // belief[v] = llr[v] + sum_e c2v[e] (ascending original check index)
 __device__ __forceinline__ float var_sum(const LearnCtx& F, int v, float base, const float* __restrict__ msg) {
   const int h = v / F.vgs, j = v - h * F.vgs;
@@ -56,8 +66,8 @@ __device__ __forceinline__ float var_sum(const LearnCtx& F, int v, float base, c
 __global__ void __launch_bounds__(kLearnThreads) nms_forward_kernel(
     const DevCode* __restrict__ Cp, int T, int L, const float* __restrict__ llr, const uint64_t* __restrict__ cw,
     long long frames, const float* __restrict__ alpha, const float* __restrict__ beta, float* __restrict__ X,
-    float* __restrict__ Bout, char* __restrict__ work, long long work_stride, float* __restrict__ loss) {
-  __shared__ float s_loss;
+    float* __restrict__ Bout, char* __restrict__ work, long long work_stride, float* __restrict__ pf) {
+  __shared__ float s_part[kLearnThreads / 32];
   const DevCode C = *Cp;
   const LearnCtx F = make_ctx(C, L);
   const int n = F.n, E = C.e_slots;
@@ -67,7 +77,6 @@ __global__ void __launch_bounds__(kLearnThreads) nms_forward_kernel(
   for (long long f = blockIdx.x; f < frames; f += gridDim.x) {
     const float* lf = llr + f * (long long)n;
     for (int v = threadIdx.x; v < n; v += blockDim.x) app[v] = lf[v];
-    if (threadIdx.x == 0) s_loss = 0.0f;
     __syncthreads();
     for (int t = 0; t < T; t++) {
       float* Xt = X + (f * T + t) * (long long)E;
@@ -123,9 +132,14 @@ __global__ void __launch_bounds__(kLearnThreads) nms_forward_kernel(
       const float z = -s * b;
       part += (z > 0.0f ? z + log1pf(expf(-z)) : log1pf(expf(z))) * scale;
     }
-    atomicAdd(&s_loss, part);
+    part = warp_sum_fixed(part);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = part;
     __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(loss, s_loss);
+    if (threadIdx.x == 0) {
+      float sum = 0.0f;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) sum = __fadd_rn(sum, s_part[w]);
+      pf[f * (2LL * T * L + 1) + 2 * T * L] = sum;
+    }
     __syncthreads();
   }
 }
@@ -134,13 +148,13 @@ __global__ void __launch_bounds__(kLearnThreads) nms_backward_kernel(
     const DevCode* __restrict__ Cp, int T, int L, const float* __restrict__ llr, const uint64_t* __restrict__ cw,
     long long frames, const float* __restrict__ alpha, const float* __restrict__ beta,
     const float* __restrict__ X, const float* __restrict__ Bin, char* __restrict__ work, long long work_stride,
-    float* __restrict__ grad_alpha, float* __restrict__ grad_beta) {
-  extern __shared__ float s_g[];  // [2 * L]: alpha then beta gradients of the current t
+    float* __restrict__ pf) {
   const DevCode C = *Cp;
   const LearnCtx F = make_ctx(C, L);
   const int n = F.n, E = C.e_slots;
   float* gx = (float*)(work + (long long)blockIdx.x * work_stride);
   float* gb = gx + ((E + 63) & ~63);
+  float* gchk = gb + ((n + 63) & ~63);  // [2][m]: per-check alpha / beta gradient terms
   const float scale = 1.0f / ((float)frames * (float)n);
   for (long long f = blockIdx.x; f < frames; f += gridDim.x) {
     const uint64_t* cf = cw + f * (long long)C.words_n;
@@ -154,8 +168,6 @@ __global__ void __launch_bounds__(kLearnThreads) nms_backward_kernel(
     }
     __syncthreads();
     for (int t = T - 1; t >= 0; t--) {
-      for (int i = threadIdx.x; i < 2 * L; i += blockDim.x) s_g[i] = 0.0f;
-      __syncthreads();
       const float* Xt = X + (f * T + t) * (long long)E;
       for (int cc = threadIdx.x; cc < F.m; cc += blockDim.x) {
         const int g = F.chk_cg[cc];
@@ -214,18 +226,46 @@ __global__ void __launch_bounds__(kLearnThreads) nms_backward_kernel(
           else if (i == i2) gxi = g2 * (Xt[s] < 0.0f ? -1.0f : 1.0f);
           gx[s] = gxi;
         }
-        if (gA != 0.0f) atomicAdd(&s_g[lay], gA);
-        if (gB != 0.0f) atomicAdd(&s_g[L + lay], gB);
+        gchk[cc] = gA;
+        gchk[F.m + cc] = gB;
       }
       __syncthreads();
-      for (int i = threadIdx.x; i < L; i += blockDim.x) {
-        if (s_g[i] != 0.0f) atomicAdd(&grad_alpha[t * L + i], s_g[i]);
-        if (s_g[L + i] != 0.0f) atomicAdd(&grad_beta[t * L + i], s_g[L + i]);
+      // per row group sums in a fixed order: warp w takes layers w, w + nwarps, ...
+      for (int lay = threadIdx.x >> 5; lay < L; lay += blockDim.x >> 5) {
+        const int c0 = (L == F.ncg) ? F.cg[lay].x : 0, c1 = (L == F.ncg) ? c0 + F.cg[lay].y : F.m;
+        float sa = 0.0f, sb = 0.0f;
+        for (int cc = c0 + (threadIdx.x & 31); cc < c1; cc += 32) {
+          sa = __fadd_rn(sa, gchk[cc]);
+          sb = __fadd_rn(sb, gchk[F.m + cc]);
+        }
+        sa = warp_sum_fixed(sa);
+        sb = warp_sum_fixed(sb);
+        if ((threadIdx.x & 31) == 0) {
+          float* row = pf + f * (2LL * T * L + 1);
+          row[t * L + lay] = sa;
+          row[T * L + t * L + lay] = sb;
+        }
       }
       if (t > 0)
         for (int v = threadIdx.x; v < n; v += blockDim.x) gb[v] = var_sum(F, v, 0.0f, gx);  // dL/db^{t-1}
       __syncthreads();
     }
+  }
+}
+
+// out[i] = sum over frames f (ascending) of pf[f][i], i < 2 T L + 1; warp per i.
+__global__ void nms_reduce_kernel(const float* __restrict__ pf, long long frames, int TL,
+                                  float* __restrict__ grad_alpha, float* __restrict__ grad_beta,
+                                  float* __restrict__ loss) {
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i > 2 * TL) return;
+  float s = 0.0f;
+  for (long long f = threadIdx.x & 31; f < frames; f += 32) s = __fadd_rn(s, pf[f * (2LL * TL + 1) + i]);
+  s = warp_sum_fixed(s);
+  if ((threadIdx.x & 31) == 0) {
+    if (i < TL) grad_alpha[i] = s;
+    else if (i < 2 * TL) grad_beta[i - TL] = s;
+    else *loss = s;
   }
 }
 
@@ -245,19 +285,23 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
 
 int launch_nms_forward(const DevCode* dcode, const DevCode& h, int T, int L, const float* llr, const uint64_t* cw,
                        long long frames, const float* alpha, const float* beta, float* X, float* B, char* work,
-                       long long work_stride, int grid, float* loss, cudaStream_t st) {
+                       long long work_stride, int grid, float* pf, cudaStream_t st) {
   if (h.max_dc > kLearnDcMax) return set_error(GF2C_ERR_UNSUPPORTED, "learned decoder: check degree above 32");
   nms_forward_kernel<<<grid, kLearnThreads, 0, st>>>(dcode, T, L, llr, cw, frames, alpha, beta, X, B, work,
-                                                     work_stride, loss);
+                                                     work_stride, pf);
   GF2C_CUDA(cudaGetLastError());
   return GF2C_OK;
 }
 
 int launch_nms_backward(const DevCode* dcode, const DevCode& h, int T, int L, const float* llr, const uint64_t* cw,
                         long long frames, const float* alpha, const float* beta, const float* X, const float* B,
-                        char* work, long long work_stride, int grid, float* ga, float* gb, cudaStream_t st) {
-  nms_backward_kernel<<<grid, kLearnThreads, 2 * L * sizeof(float), st>>>(dcode, T, L, llr, cw, frames, alpha, beta,
-                                                                          X, B, work, work_stride, ga, gb);
+                        char* work, long long work_stride, int grid, float* pf, float* ga, float* gb,
+                        float* loss, cudaStream_t st) {
+  nms_backward_kernel<<<grid, kLearnThreads, 0, st>>>(dcode, T, L, llr, cw, frames, alpha, beta, X, B, work,
+                                                      work_stride, pf);
+  GF2C_CUDA(cudaGetLastError());
+  const int outs = 2 * T * L + 1, warps = 8;
+  nms_reduce_kernel<<<(outs + warps - 1) / warps, warps * 32, 0, st>>>(pf, frames, T * L, ga, gb, loss);
   GF2C_CUDA(cudaGetLastError());
   return GF2C_OK;
 }

@@ -29,10 +29,10 @@
 // posteriors and every variable group reads contiguous check states.
 //
 // Placement.  The check states (m x 16 B) and the posteriors (n x 4 B) live in
-// shared memory when they fit together (DVB-T2 short frames); otherwise each
-// lives in the CTA's global workspace slice, which stays in the 126 MB L2 for
-// the frames in flight.  The u-order copy of the channel LLRs (read once per
-// iteration) is always in the workspace.
+// shared memory when they fit together (DVB-T2 short frames, ALL_SMEM);
+// otherwise both live in the CTA's global workspace slice, which the L1 and the
+// 126 MB L2 cache for the frames in flight.  The u-order copy of the channel
+// LLRs (read once per iteration) is in the workspace.
 #include <cuda_fp16.h>
 
 #include "internal.h"
@@ -52,52 +52,206 @@ __device__ __forceinline__ float round_mag16(float v) {
   return __half2float(__float2half_rn(v > 65504.0f ? 65504.0f : v));
 }
 
-// u-order variable of slot descriptor D for check t of a row group of Z checks
-__device__ __forceinline__ int state_desc_var(uint32_t D, int t, int Z) {
-  const int base = (int)(D & 0xFFFFFu), sh = (int)((D >> 20) & 1023u);
-  const int c = t + sh;
-  const int u = base + (c >= Z ? c - Z : c);
-  return ((D >> 31) && t == 0) ? -1 : u;
-}
+// Posteriors in u order (shared memory or the CTA workspace).
+template <bool ALL_SMEM>
+struct Post {
+  float* p;
+  __device__ __forceinline__ float* at(int u) const { return p + u; }
+  __device__ __forceinline__ float* run(int) const { return p; }
+};
 
-// Posteriors of the slots of check t of row group G (slot i in ap[i]); returns
-// the mask of the slots that hold an edge.
-template <int DCMAX>
-__device__ __forceinline__ uint32_t load_slots(const DevCode& C, const int4 G, int t, const float* app,
-                                               float (&ap)[DCMAX]) {
-  uint32_t real = 0;
-  if (C.sp_desc) {
-    const uint32_t* __restrict__ sd = C.sp_desc + G.w;
+struct SlotTables {
+  const int2* desc;      // DevCode::sp_desc
+  const uint32_t* absent;
+  const int* slot_var;
+};
+
+// Posteriors of the slots of check t of row group g (slot i in ap[i]); returns
+// the mask of the slots that hold an edge.  Every address is valid, so the
+// loads are issued unconditionally, back to back.
+template <int DCMAX, bool ALL_SMEM>
+__device__ __forceinline__ uint32_t load_slots(const SlotTables T, int g, const int4 G, int t, uint32_t dmask,
+                                               const Post<ALL_SMEM> P, float (&ap)[DCMAX]) {
+  if (T.desc) {
+    const int2* __restrict__ sd = T.desc + G.w;
 #pragma unroll
     for (int i = 0; i < DCMAX; i++) {
       if (i < G.z) {
-        const int u = state_desc_var(__ldg(&sd[i]), t, G.y);
-        real |= (uint32_t)(u >= 0) << i;
-        ap[i] = app[u < 0 ? 0 : u];
+        const int2 D = __ldg(&sd[i]);
+        ap[i] = P.run(D.x)[D.x + t - (t >= D.y ? G.y : 0)];
       }
     }
-  } else {
-    const int* __restrict__ sv = C.slot_var + G.w + t;
+    return t == 0 ? dmask & ~__ldg(&T.absent[g]) : dmask;
+  }
+  const int* __restrict__ sv = T.slot_var + G.w + t;
+  uint32_t real = 0;
 #pragma unroll
-    for (int i = 0; i < DCMAX; i++) {
-      if (i < G.z) {
-        const int u = __ldg(&sv[i * G.y]);
-        real |= (uint32_t)(u >= 0) << i;
-        ap[i] = app[u < 0 ? 0 : u];
-      }
+  for (int i = 0; i < DCMAX; i++) {
+    if (i < G.z) {
+      const int u = __ldg(&sv[i * G.y]);
+      real |= (uint32_t)(u >= 0) << i;
+      ap[i] = *P.at(u < 0 ? 0 : u);
     }
   }
   return real;
+}
+
+// Check-node update from the slot posteriors ap[] and the old state `so`:
+// writes the new state and returns the parity of the hard decisions of the
+// posteriors.  ALLREAL: every slot below d holds an edge; FIRST: the old
+// messages are all zero.
+template <int DCMAX, bool FIRST, bool ALLREAL>
+__device__ __forceinline__ int check_node(const float (&ap)[DCMAX], uint32_t real, int d, const uint4 so,
+                                          uint4* st_cc, bool nms, float al, float be, bool msg16) {
+  float m1 = __int_as_float(0x7f800000), m2 = m1;
+  uint32_t i1 = 0xffu, neg = 0u;
+  int hp = 0;
+#pragma unroll
+  for (int i = 0; i < DCMAX; i++) {
+    if (i < d && (ALLREAL || ((real >> i) & 1u))) {
+      hp ^= (int)(ap[i] < 0.0f);
+      const float x = FIRST ? ap[i] : __fsub_rn(ap[i], state_c2v(so, i));
+      const float ax = fabsf(x);
+      const bool lt1 = ax < m1, lt2 = ax < m2;
+      m2 = lt1 ? m1 : (lt2 ? ax : m2);
+      m1 = lt1 ? ax : m1;
+      i1 = lt1 ? (uint32_t)i : i1;
+      neg |= (uint32_t)(x < 0.0f) << i;
+    }
+  }
+  const bool single = ALLREAL ? d == 1 : __popc(real) == 1;
+  float mag1 = single ? 0.0f : m1, mag2 = single ? 0.0f : m2;
+  if (nms) {  // normalised / offset min-sum
+    const float d1 = __fsub_rn(mag1, be), d2 = __fsub_rn(mag2, be);
+    mag1 = __fmul_rn(al, d1 > 0.0f ? d1 : 0.0f);
+    mag2 = __fmul_rn(al, d2 > 0.0f ? d2 : 0.0f);
+  }
+  if (msg16) {
+    mag1 = round_mag16(mag1);
+    mag2 = round_mag16(mag2);
+  }
+  const uint32_t sgn = (__popc(neg) & 1) ? ~neg : neg;
+  *st_cc = make_uint4(__float_as_uint(mag1), __float_as_uint(mag2), sgn, i1);
+  return hp;
+}
+
+// The code descriptor of the frame a CTA is decoding (shared by the passes).
+__shared__ DevCode sf_code;
+
+// Check-node pass: every check reads its slot posteriors and its old state and
+// writes its new state.  Returns this thread's part of the parity of the hard
+// decisions over all checks (the syndrome of the previous iteration).  NMS
+// weights of this iteration start at alpha / beta + nms_row, one per row group
+// when per_layer, else one for the whole code.
+template <int DCMAX, bool ALL_SMEM>
+__device__ __forceinline__ int sf_check_pass(uint4* st, const Post<ALL_SMEM> P, bool first, bool nms, bool msg16,
+                                             const float* alpha, const float* beta, int nms_row, bool per_layer) {
+  const DevCode& C = sf_code;
+  const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const SlotTables T{C.sp_desc, C.sp_absent, C.slot_var};
+  const int2* __restrict__ cch = C.sp_cchunk;
+  const int4* __restrict__ spcg = C.sp_cg;
+  const int ncc = C.sp_ncchunk;
+  int par = 0;
+  for (int ch = threadIdx.x >> 5; ch < ncc; ch += nwarps) {
+    const int2 CH = cch[ch];
+    const int4 G = spcg[CH.x];
+    const int t = CH.y + lane;
+    if (t >= G.y) continue;
+    const int cc = G.x + t;
+    const uint32_t dmask = G.z >= 32 ? 0xffffffffu : (1u << G.z) - 1u;
+    float ap[DCMAX];
+    const uint32_t real = load_slots<DCMAX, ALL_SMEM>(T, CH.x, G, t, dmask, P, ap);
+    float al = 1.0f, be = 0.0f;
+    if (nms) {
+      const int idx = nms_row + (per_layer ? CH.x : 0);
+      al = __ldg(&alpha[idx]);
+      be = __ldg(&beta[idx]);
+    }
+    if (real == dmask) {
+      if (first)
+        par |= check_node<DCMAX, true, true>(ap, real, G.z, make_uint4(0u, 0u, 0u, 0xffu), st + cc, nms, al, be,
+                                             msg16);
+      else
+        par |= check_node<DCMAX, false, true>(ap, real, G.z, st[cc], st + cc, nms, al, be, msg16);
+    } else {
+      const uint4 so = first ? make_uint4(0u, 0u, 0u, 0xffu) : st[cc];
+      par |= check_node<DCMAX, false, false>(ap, real, G.z, so, st + cc, nms, al, be, msg16);
+    }
+  }
+  return par;
+}
+
+// Variable-node pass: belief = llr + sum of c2v in ascending original check index.
+template <bool ALL_SMEM>
+__device__ __forceinline__ void sf_var_pass(const uint4* st, const Post<ALL_SMEM> P, const float* lu) {
+  const DevCode& C = sf_code;
+  const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int nvc = C.sp_nvchunk, vgs = C.vgs, n = C.n;
+  const int2* __restrict__ vch = C.sp_vchunk;
+  const int2* __restrict__ svg = C.sp_vg;
+  const int* __restrict__ sci = C.sp_ci;
+  for (int ch = threadIdx.x >> 5; ch < nvc; ch += nwarps) {
+    const int2 CH = vch[ch];
+    const int2 V = svg[CH.x];
+    const int j = CH.y + lane;
+    const int u = CH.x * vgs + j;
+    if (j >= vgs || u >= n) continue;
+    float b = lu[u];
+    {
+      const int* __restrict__ ci = sci + V.y + j;
+      int i = 0;
+      for (; i + 4 <= V.x; i += 4) {
+        int e[4];
+        uint4 s[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) e[q] = __ldg(&ci[(i + q) * vgs]);
+#pragma unroll
+        for (int q = 0; q < 4; q++) s[q] = st[e[q] < 0 ? 0 : (e[q] & 0xffffff)];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if (e[q] >= 0) b = __fadd_rn(b, state_c2v(s[q], e[q] >> 24));
+      }
+      for (; i < V.x; i++) {
+        const int e0 = __ldg(&ci[i * vgs]);
+        if (e0 >= 0) b = __fadd_rn(b, state_c2v(st[e0 & 0xffffff], e0 >> 24));
+      }
+    }
+    *P.at(u) = b;
+  }
+}
+
+// Parity of the hard decisions over all checks (this thread's part).
+template <int DCMAX, bool ALL_SMEM>
+__device__ __forceinline__ int sf_syndrome_pass(const Post<ALL_SMEM> P) {
+  const DevCode& C = sf_code;
+  const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const SlotTables T{C.sp_desc, C.sp_absent, C.slot_var};
+  int p = 0;
+  for (int ch = threadIdx.x >> 5; ch < C.sp_ncchunk; ch += nwarps) {
+    const int2 CH = C.sp_cchunk[ch];
+    const int4 G = C.sp_cg[CH.x];
+    const int t = CH.y + lane;
+    if (t >= G.y) continue;
+    float ap[DCMAX];
+    const uint32_t real =
+        load_slots<DCMAX, ALL_SMEM>(T, CH.x, G, t, G.z >= 32 ? 0xffffffffu : (1u << G.z) - 1u, P, ap);
+#pragma unroll
+    for (int i = 0; i < DCMAX; i++)
+      if (i < G.z && ((real >> i) & 1u)) p ^= (int)(ap[i] < 0.0f);
+  }
+  return p;
 }
 
 template <int DCMAX, bool ALL_SMEM>
 __global__ void __launch_bounds__(kStateThreads, 1) bp_state_flood_kernel(const DecodeArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ long long s_frame;
-  __shared__ DevCode C;
-  const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = NT >> 5;
+  const DevCode& C = sf_code;
+  const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31;
   char* work = a.work + (long long)blockIdx.x * a.work_stride;
-  const bool msg16 = a.sf_msg16 != 0;  // magnitudes rounded to binary16
+  uint4* st = ALL_SMEM ? (uint4*)smem_raw : (uint4*)(work + a.sf_st_off);
+  const Post<ALL_SMEM> P{ALL_SMEM ? (float*)(smem_raw + a.sf_app_soff) : (float*)(work + a.sf_app_off)};
   for (;;) {
     if (tid == 0) s_frame = (long long)atomicAdd(a.queue, 1ull);
     __syncthreads();
@@ -112,22 +266,10 @@ __global__ void __launch_bounds__(kStateThreads, 1) bp_state_flood_kernel(const 
       __syncthreads();
       continue;
     }
-    if (tid == 0) C = a.codes[cid];
+    if (tid == 0) sf_code = a.codes[cid];
     __syncthreads();
-    const int n = C.n, m = C.m, k = C.k, vgs = C.vgs;
-    uint4* st;
-    float* app;
-    if (ALL_SMEM) {
-      st = (uint4*)smem_raw;
-      app = (float*)(smem_raw + (size_t)m * 16);
-    } else {
-      st = a.sf_st_smem ? (uint4*)smem_raw : (uint4*)(work + a.sf_st_off);
-      app = a.sf_app_smem ? (float*)(smem_raw + (a.sf_st_smem ? (size_t)m * 16 : 0)) : (float*)(work + a.sf_app_off);
-    }
+    const int n = C.n;
     const float* __restrict__ llr = a.llr + (a.llr_off ? a.llr_off[f] : f * (long long)n);
-    const int* __restrict__ u2v = C.sp_u2v;
-    float* llr_u = (float*)(work + a.sf_llr_off);
-    const float* __restrict__ lu = u2v ? llr_u : llr;
     const int maxit = a.max_iter_arr ? a.max_iter_arr[f] : a.max_iter;
     uint64_t* mo = a.msg ? a.msg + (a.msg_off ? a.msg_off[f] : f * (long long)C.words_k) : nullptr;
     float* bo = a.beliefs ? a.beliefs + (a.llr_off ? a.llr_off[f] : f * (long long)n) : nullptr;
@@ -145,138 +287,48 @@ __global__ void __launch_bounds__(kStateThreads, 1) bp_state_flood_kernel(const 
       __syncthreads();
       continue;
     }
+    const int* __restrict__ u2v = C.sp_u2v;
+    float* llr_u = (float*)(work + a.sf_llr_off);
     for (int u = tid; u < n; u += NT) {
       const float x = u2v ? llr[__ldg(&u2v[u])] : llr[u];
       if (u2v) llr_u[u] = x;
-      app[u] = x;
+      *P.at(u) = x;
     }
+    const float* lu = u2v ? llr_u : llr;
     __syncthreads();
 
-    const int4* __restrict__ spcg = C.sp_cg;
-    const int2* __restrict__ cch = C.sp_cchunk;
-    const int2* __restrict__ vch = C.sp_vchunk;
-    const int2* __restrict__ svg = C.sp_vg;
-    const int* __restrict__ sci = C.sp_ci;
-    const int ncc = C.sp_ncchunk, nvc = C.sp_nvchunk;
+    const bool nms = a.nms_iters > 0;
     int it = 0, converged = 0, synd = 1;
     for (;;) {
-      const bool first = it == 0;
-      const int tw = (a.nms_iters > 0) ? min(it, a.nms_iters - 1) : 0;
-      int par = 0;
-      // check nodes: new state from the posteriors and the old state
-      for (int ch = warp; ch < ncc; ch += nwarps) {
-        const int2 CH = cch[ch];
-        const int4 G = spcg[CH.x];
-        const int t = CH.y + lane;
-        if (t >= G.y) continue;
-        const int cc = G.x + t;
-        float ap[DCMAX];
-        const uint32_t real = load_slots<DCMAX>(C, G, t, app, ap);
-        const uint4 so = first ? make_uint4(0u, 0u, 0u, 0xffu) : st[cc];
-        float m1 = __int_as_float(0x7f800000), m2 = m1;
-        uint32_t i1 = 0xffu, neg = 0u;
-        int hp = 0;
-#pragma unroll
-        for (int i = 0; i < DCMAX; i++) {
-          if (i < G.z && ((real >> i) & 1u)) {
-            hp ^= (int)(ap[i] < 0.0f);
-            const float x = __fsub_rn(ap[i], state_c2v(so, i));
-            const float ax = fabsf(x);
-            const bool lt1 = ax < m1, lt2 = ax < m2;
-            m2 = lt1 ? m1 : (lt2 ? ax : m2);
-            m1 = lt1 ? ax : m1;
-            i1 = lt1 ? (uint32_t)i : i1;
-            neg |= (uint32_t)(x < 0.0f) << i;
-          }
-        }
-        par |= hp;
-        const bool single = __popc(real) == 1;
-        float mag1 = single ? 0.0f : m1, mag2 = single ? 0.0f : m2;
-        if (a.nms_iters > 0) {  // normalised / offset min-sum
-          const int lay = (a.nms_L == C.ncg) ? CH.x : 0;
-          const float al = __ldg(&a.alpha[tw * a.nms_L + lay]), be = __ldg(&a.beta[tw * a.nms_L + lay]);
-          const float d1 = __fsub_rn(mag1, be), d2 = __fsub_rn(mag2, be);
-          mag1 = __fmul_rn(al, d1 > 0.0f ? d1 : 0.0f);
-          mag2 = __fmul_rn(al, d2 > 0.0f ? d2 : 0.0f);
-        }
-        if (msg16) {
-          mag1 = round_mag16(mag1);
-          mag2 = round_mag16(mag2);
-        }
-        const uint32_t sgn = (__popc(neg) & 1) ? ~neg : neg;
-        st[cc] = make_uint4(__float_as_uint(mag1), __float_as_uint(mag2), sgn, i1);
-      }
+      const int nms_row = nms ? min(it, a.nms_iters - 1) * a.nms_L : 0;
+      int par = sf_check_pass<DCMAX, ALL_SMEM>(st, P, it == 0, nms, a.sf_msg16 != 0, a.alpha, a.beta, nms_row,
+                                               a.nms_L == C.ncg);
       par = __syncthreads_or(par);
       if (it > 0 && a.early_stop && !par) {
         converged = 1;
         synd = 0;
         break;
       }
-      // variable nodes: belief = llr + sum of c2v in ascending original check index
-      for (int ch = warp; ch < nvc; ch += nwarps) {
-        const int2 CH = vch[ch];
-        const int2 V = svg[CH.x];
-        const int j = CH.y + lane;
-        const int u = CH.x * vgs + j;
-        if (j >= vgs || u >= n) continue;
-        const int* __restrict__ ci = sci + V.y + j;
-        float b = lu[u];
-        int i = 0;
-        for (; i + 4 <= V.x; i += 4) {
-          int e[4];
-          uint4 s[4];
-#pragma unroll
-          for (int q = 0; q < 4; q++) e[q] = __ldg(&ci[(i + q) * vgs]);
-#pragma unroll
-          for (int q = 0; q < 4; q++) s[q] = st[e[q] < 0 ? 0 : (e[q] & 0xffffff)];
-#pragma unroll
-          for (int q = 0; q < 4; q++)
-            if (e[q] >= 0) b = __fadd_rn(b, state_c2v(s[q], e[q] >> 24));
-        }
-        if (V.x - i >= 2) {
-          const int e0 = __ldg(&ci[i * vgs]), e1 = __ldg(&ci[(i + 1) * vgs]);
-          const uint4 s0 = st[e0 < 0 ? 0 : (e0 & 0xffffff)], s1 = st[e1 < 0 ? 0 : (e1 & 0xffffff)];
-          if (e0 >= 0) b = __fadd_rn(b, state_c2v(s0, e0 >> 24));
-          if (e1 >= 0) b = __fadd_rn(b, state_c2v(s1, e1 >> 24));
-          i += 2;
-        }
-        if (i < V.x) {
-          const int e0 = __ldg(&ci[i * vgs]);
-          if (e0 >= 0) b = __fadd_rn(b, state_c2v(st[e0 & 0xffffff], e0 >> 24));
-        }
-        app[u] = b;
-      }
+      sf_var_pass<ALL_SMEM>(st, P, lu);
       __syncthreads();
       ++it;
       if (it >= maxit) break;
     }
     if (!converged) {
-      // syndrome of the final hard decisions
-      int p = 0;
-      for (int ch = warp; ch < ncc; ch += nwarps) {
-        const int2 CH = cch[ch];
-        const int4 G = spcg[CH.x];
-        const int t = CH.y + lane;
-        if (t >= G.y) continue;
-        float ap[DCMAX];
-        const uint32_t real = load_slots<DCMAX>(C, G, t, app, ap);
-#pragma unroll
-        for (int i = 0; i < DCMAX; i++)
-          if (i < G.z && ((real >> i) & 1u)) p ^= (int)(ap[i] < 0.0f);
-      }
-      synd = __syncthreads_or(p);
+      synd = __syncthreads_or(sf_syndrome_pass<DCMAX, ALL_SMEM>(P));
       converged = !synd;
     }
     if (mo) {  // message bits: the first k variables (identical in u order)
       uint32_t* mo32 = (uint32_t*)mo;
-      for (int base = 0; base < 64 * C.words_k; base += NT) {
+      const int k = C.k, wk = C.words_k;
+      for (int base = 0; base < 64 * wk; base += NT) {
         const int u = base + tid;
-        const unsigned bits = __ballot_sync(0xffffffffu, u < k && app[u < n ? u : 0] < 0.0f);
-        if (lane == 0 && u < 64 * C.words_k) mo32[u >> 5] = bits;
+        const unsigned bits = __ballot_sync(0xffffffffu, u < k && *P.at(u < n ? u : 0) < 0.0f);
+        if (lane == 0 && u < 64 * wk) mo32[u >> 5] = bits;
       }
     }
     if (bo)
-      for (int u = tid; u < n; u += NT) bo[u2v ? __ldg(&u2v[u]) : u] = app[u];
+      for (int u = tid; u < n; u += NT) bo[u2v ? __ldg(&u2v[u]) : u] = *P.at(u);
     if (tid == 0) {
       if (a.iters) a.iters[f] = it;
       if (a.conv) a.conv[f] = (uint8_t)converged;
@@ -285,6 +337,8 @@ __global__ void __launch_bounds__(kStateThreads, 1) bp_state_flood_kernel(const 
     __syncthreads();
   }
 }
+
+int state_flood_threads() { return kStateThreads; }
 
 int state_dcmax_bucket(int max_dc) {
   static const int buckets[] = {7, 9, 10, 11, 13, 14, 18, 19, 22, 26, 32};
