@@ -294,8 +294,8 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   for (int i = 0; i < ncodes; i++) {
     if (!codes[i]) return set_error(GF2C_ERR_INVALID_ARG, "NULL code handle");
     const HostCode& h = *codes[i]->h;
-    if (o.schedule == GF2C_SCHED_LAYERED && !h.layered_ok)
-      return set_error(GF2C_ERR_UNSUPPORTED, "layered schedule needs a QC or DVB-T2 code with Z <= 1024");
+    if (o.schedule == GF2C_SCHED_LAYERED && (!h.layered_ok || h.sp_desc.empty()))
+      return set_error(GF2C_ERR_UNSUPPORTED, "layered schedule needs a QC or DVB-T2 code with Z <= 1023");
     int rc = ensure_code_on_device(codes[i]);
     if (rc) return rc;
     d->codes.push_back(codes[i]);

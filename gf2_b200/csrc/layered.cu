@@ -8,10 +8,12 @@
 // adds (c2v_new - c2v_old) to the APP of its variables.
 //
 // One CTA decodes one frame at a time (persistent, frames from an atomic
-// queue), one thread per check of the row group.  The variable of every slot is
-// computed from a per-row-group slot descriptor shared by all checks (circulant
-// base + (t + shift) mod Z, or the DVB-T2 staircase), so no index table is read
-// in the hot loop.  All loads of a check are issued back to back from
+// queue), one thread per check of the row group.  The posteriors are kept in
+// the u order of the check-state plan (DVB-T2 parity bit k + a + q t at
+// k + a Z + t), where every slot of a row group is a rotated run of Z
+// consecutive variables: check t reads start + t - (t >= wrap ? Z : 0) from a
+// per-(row group, slot) descriptor, so no index table is read in the hot loop
+// and every slot load of a warp is coalesced.  All loads of a check are issued back to back from
 // always-valid addresses before any arithmetic (memory-level parallelism), and
 // then the check node, the message stores and the APP updates follow.
 //
@@ -82,29 +84,24 @@ struct LayerSmem {
   int* unsat;         // number of unsatisfied checks
 };
 
-// Variable of packed slot descriptor D for check t of row group g (Z checks).
-__device__ __forceinline__ int slot_var_of(uint32_t D, int t, int Z, int g) {
-  const int base = (int)(D & 0xFFFFFu), sh = (int)((D >> 20) & 1023u), type = (int)(D >> 30);
-  if (type == 0) {
-    const int c = t + sh;
-    return base + (c >= Z ? c - Z : c);
-  }
-  const int v = base + sh * t;
-  if (type == 1) return (g == 0 && t == 0) ? -1 : v - 1;
-  return v;
-}
+// u-order variable of slot descriptor D = {start, wrap} for check t of a row
+// group of Z checks (every result is a valid index; a slot without an edge at
+// t = 0 is masked separately).
+__device__ __forceinline__ int slot_u(const int2 D, int t, int Z) { return D.x + t - (t >= D.y ? Z : 0); }
 
-// A hard decision flipped: toggle it and the parity of the variable's checks,
-// and update the number of unsatisfied checks (rare after the first iterations).
-__device__ __noinline__ void flip_var(int v, const LayerSmem S, const int2* __restrict__ vg,
-                                      const int* __restrict__ vg_chk, int vgs) {
-  atomicXor(&S.bitmap[v >> 5], 1u << (v & 31));
-  const int h = v / vgs, j = v - h * vgs;
+// A hard decision flipped: toggle it and the parity of the variable's checks
+// (u-order edge lists, flattened check | slot << 24), and update the number of
+// unsatisfied checks (rare after the first iterations).
+__device__ __noinline__ void flip_var(int u, const LayerSmem S, const int2* __restrict__ vg,
+                                      const int* __restrict__ ci, int vgs) {
+  atomicXor(&S.bitmap[u >> 5], 1u << (u & 31));
+  const int h = u / vgs, j = u - h * vgs;
   const int2 V = vg[h];
   int delta = 0;
   for (int i = 0; i < V.x; i++) {
-    const int cc = __ldg(&vg_chk[V.y + i * vgs + j]);
-    if (cc < 0) break;
+    const int e = __ldg(&ci[V.y + i * vgs + j]);
+    if (e < 0) break;
+    const int cc = e & 0xffffff;
     const uint32_t was = atomicXor(&S.chkpar[cc >> 5], 1u << (cc & 31));
     delta += ((was >> (cc & 31)) & 1u) ? -1 : 1;
   }
@@ -155,11 +152,13 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
     __syncthreads();
     const int n = C.n, m = C.m, vgs = C.vgs, ncg = C.ncg;
     const int4* __restrict__ cgp = C.cg;
+    const int4* __restrict__ spcg = C.sp_cg;
     const uint32_t* __restrict__ cgs = C.cg_sync;
-    const int* __restrict__ slot_var = C.slot_var;
-    const uint32_t* __restrict__ sdesc = C.slot_desc;
-    const int2* __restrict__ vg = C.vg;
-    const int* __restrict__ vg_chk = C.vg_chk;
+    const int2* __restrict__ sdesc = C.sp_desc;
+    const uint32_t* __restrict__ absent = C.sp_absent;
+    const int* __restrict__ u2v = C.sp_u2v;
+    const int2* __restrict__ vg = C.sp_vg;
+    const int* __restrict__ vg_chk = C.sp_ci;
     const float* __restrict__ llr = a.llr + (a.llr_off ? a.llr_off[f] : f * (long long)n);
     const int maxit = a.max_iter_arr ? a.max_iter_arr[f] : a.max_iter;
     float* app = (n <= a.smem_app_floats) ? smem_app : gapp;
@@ -180,16 +179,16 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
       continue;
     }
 
-    // APP = llr; hard decisions
+    // APP = llr (u order); hard decisions
     for (int base = 0; base < n; base += NT) {
-      const int v = base + tid;
+      const int u = base + tid;
       float x = 0.0f;
-      if (v < n) {
-        x = __ldcs(llr + v);
-        app[v] = x;
+      if (u < n) {
+        x = u2v ? llr[__ldg(&u2v[u])] : __ldcs(llr + u);
+        app[u] = x;
       }
-      const unsigned b = __ballot_sync(0xffffffffu, v < n && x < 0.0f);
-      if ((tid & 31) == 0 && v < n) bitmap[v >> 5] = b;
+      const unsigned b = __ballot_sync(0xffffffffu, u < n && x < 0.0f);
+      if ((tid & 31) == 0 && u < n) bitmap[u >> 5] = b;
     }
     __syncthreads();
     // check parities and the unsatisfied count
@@ -200,11 +199,12 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
         uint32_t p = 0;
         if (cc < m) {
           const int g = C.chk_cg[cc];
-          const int4 G = cgp[g];
+          const int4 G = spcg[g];
           const int t = cc - G.x;
+          const uint32_t ab = t == 0 ? __ldg(&absent[g]) : 0u;
           for (int i = 0; i < G.z; i++) {
-            const int v = __ldg(&slot_var[G.w + i * G.y + t]);
-            if (v >= 0) p ^= (bitmap[v >> 5] >> (v & 31)) & 1u;
+            const int u = slot_u(__ldg(&sdesc[G.w + i]), t, G.y);
+            if (!((ab >> i) & 1u)) p ^= (bitmap[u >> 5] >> (u & 31)) & 1u;
           }
         }
         cnt += (int)p;
@@ -226,14 +226,16 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
         const int d = G.z, nchk = G.y;
         const int t = act ? tid : 0;
         const int s0 = G.w + t;
-        const uint32_t* __restrict__ sd = sdesc + G.w / nchk;
+        const int2* __restrict__ sd = sdesc + spcg[g].w;
         int vv[DCMAX];
         float ap[DCMAX], o[DCMAX], w[DCMAX];
         uint32_t real = 0, neg = 0, apneg = 0;
         if (act) {
           // 1. indices, 2. all loads, 3. arithmetic
+          const uint32_t ab = t == 0 ? __ldg(&absent[g]) : 0u;
 #pragma unroll
-          for (int i = 0; i < DCMAX; i++) vv[i] = (i < d) ? slot_var_of(__ldg(&sd[i]), t, nchk, g) : -1;
+          for (int i = 0; i < DCMAX; i++)
+            vv[i] = (i < d && !((ab >> i) & 1u)) ? slot_u(__ldg(&sd[i]), t, nchk) : -1;
 #pragma unroll
           for (int i = 0; i < DCMAX; i++) ap[i] = app[vv[i] < 0 ? 0 : vv[i]];
           if (first) {
@@ -373,7 +375,7 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
       }
     }
     if (bo)
-      for (int v = tid; v < n; v += NT) bo[v] = app[v];
+      for (int u = tid; u < n; u += NT) bo[u2v ? __ldg(&u2v[u]) : u] = app[u];
     if (tid == 0) {
       if (a.iters) a.iters[f] = it;
       if (a.conv) a.conv[f] = (uint8_t)converged;
