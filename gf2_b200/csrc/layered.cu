@@ -114,6 +114,56 @@ __device__ __forceinline__ void app_put(float* app, int v, bool old_neg, float n
   if (old_neg != (nw < 0.0f)) flip_var(v, S, vg, vg_chk, vgs);
 }
 
+// Fast sum-product update of check t of a row group whose D slots all hold an
+// edge and whose variables are all distinct (the common case): loads, check
+// node, message stores and posterior updates in one pass; flipped hard
+// decisions are collected in a mask and handled after the loop (one call
+// site).  Same arithmetic as the general path of bp_layered_kernel.
+template <int MSG16, int D>
+__device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
+                                             typename MsgIO<MSG16>::T* __restrict__ c2v, bool first,
+                                             const LayerSmem& S, const int2* __restrict__ vg,
+                                             const int* __restrict__ ci, int vgs) {
+  typedef MsgIO<MSG16> IO;
+  float x[D], e[D];
+#pragma unroll
+  for (int i = 0; i < D; i++) x[i] = app[slot_u(__ldg(&sd[i]), t, nchk)];
+  uint32_t neg = 0, apneg = 0;
+#pragma unroll
+  for (int i = 0; i < D; i++) apneg |= (uint32_t)(x[i] < 0.0f) << i;
+  if (!first) {
+#pragma unroll
+    for (int i = 0; i < D; i++) x[i] = __fsub_rn(x[i], ld_msg<MSG16>(c2v, s0 + i * nchk));
+  }
+  float N = 1.0f, Dp = 1.0f;
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    neg |= (uint32_t)(x[i] < 0.0f) << i;
+    e[i] = ex2_approx(fabsf(x[i]) * -1.4426950408889634f);
+    N *= fmaxf(1.0f - e[i], 5.9604645e-08f);
+    Dp = __fmaf_rn(Dp, e[i], Dp);
+  }
+  const uint32_t negp = __popc(neg) & 1u;
+  uint32_t flips = 0;
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    const float ni = fmaxf(1.0f - e[i], 5.9604645e-08f), di = 1.0f + e[i];
+    const float num = __fmaf_rn(Dp, ni, N * di);
+    const float den = fmaxf(__fmaf_rn(Dp, ni, -N * di), num * 5.9604645e-08f);
+    const float mag = fminf(0.69314718055994531f * lg2_approx(num * rcp_approx(den)), 16.635532f);
+    const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
+    st_msg<MSG16>(c2v, s0 + i * nchk, out);
+    const float nw = x[i] + out;
+    app[slot_u(__ldg(&sd[i]), t, nchk)] = nw;
+    flips |= (uint32_t)(((apneg >> i) & 1u) != (uint32_t)(nw < 0.0f)) << i;
+  }
+  while (flips) {  // rare after the first iterations
+    const int i = __ffs(flips) - 1;
+    flips &= flips - 1;
+    flip_var(slot_u(__ldg(&sd[i]), t, nchk), S, vg, ci, vgs);
+  }
+}
+
 template <int ALGO, int MSG16, int DCMAX, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs a) {
   typedef typename MsgIO<MSG16>::T MsgT;
@@ -230,9 +280,11 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
         int vv[DCMAX];
         float ap[DCMAX], o[DCMAX], w[DCMAX];
         uint32_t real = 0, neg = 0, apneg = 0;
-        if (act) {
+        const uint32_t ab = (act && t == 0) ? __ldg(&absent[g]) : 0u;
+        if (ALGO == L_SPA_FAST && DCMAX <= 16 && act && sync == 0 && d == DCMAX && ab == 0) {
+          spa_fast_row<MSG16, DCMAX>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs);
+        } else if (act) {
           // 1. indices, 2. all loads, 3. arithmetic
-          const uint32_t ab = t == 0 ? __ldg(&absent[g]) : 0u;
 #pragma unroll
           for (int i = 0; i < DCMAX; i++)
             vv[i] = (i < d && !((ab >> i) & 1u)) ? slot_u(__ldg(&sd[i]), t, nchk) : -1;
@@ -385,31 +437,48 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
   }
 }
 
-template <int ALGO, int MSG16, int MAXT, int MINB>
-static const void* lay_dc(int dcmax) {
+// Row groups of up to 384 checks: one kernel per slot count of the DVB-T2
+// codes (an exact fit wastes no slot and keeps the all-edges fast path).
+template <int ALGO, int MSG16, int MINB>
+static const void* lay_exact(int dcmax) {
   switch (dcmax) {
-    case 8: return (const void*)bp_layered_kernel<ALGO, MSG16, 8, MAXT, MINB>;
-    case 12: return (const void*)bp_layered_kernel<ALGO, MSG16, 12, MAXT, MINB>;
-    case 16: return (const void*)bp_layered_kernel<ALGO, MSG16, 16, MAXT, MINB>;
-    case 24: return (const void*)bp_layered_kernel<ALGO, MSG16, 24, MAXT, MINB>;
-    case 32: return (const void*)bp_layered_kernel<ALGO, MSG16, 32, MAXT, MINB>;
+    case 7: return (const void*)bp_layered_kernel<ALGO, MSG16, 7, 384, MINB>;
+    case 9: return (const void*)bp_layered_kernel<ALGO, MSG16, 9, 384, MINB>;
+    case 10: return (const void*)bp_layered_kernel<ALGO, MSG16, 10, 384, MINB>;
+    case 11: return (const void*)bp_layered_kernel<ALGO, MSG16, 11, 384, MINB>;
+    case 13: return (const void*)bp_layered_kernel<ALGO, MSG16, 13, 384, MINB>;
+    case 14: return (const void*)bp_layered_kernel<ALGO, MSG16, 14, 384, MINB>;
+    case 18: return (const void*)bp_layered_kernel<ALGO, MSG16, 18, 384, MINB>;
+    case 19: return (const void*)bp_layered_kernel<ALGO, MSG16, 19, 384, MINB>;
+    case 22: return (const void*)bp_layered_kernel<ALGO, MSG16, 22, 384, MINB>;
+    case 26: return (const void*)bp_layered_kernel<ALGO, MSG16, 26, 384, MINB>;
+    case 32: return (const void*)bp_layered_kernel<ALGO, MSG16, 32, 384, MINB>;
   }
+  return nullptr;
+}
+
+// Row groups of up to 1024 checks (generic QC codes): coarser slot buckets.
+template <int ALGO, int MSG16>
+static const void* lay_wide(int dcmax) {
+  if (dcmax <= 8) return (const void*)bp_layered_kernel<ALGO, MSG16, 8, 1024, 1>;
+  if (dcmax <= 12) return (const void*)bp_layered_kernel<ALGO, MSG16, 12, 1024, 1>;
+  if (dcmax <= 16) return (const void*)bp_layered_kernel<ALGO, MSG16, 16, 1024, 1>;
+  if (dcmax <= 24) return (const void*)bp_layered_kernel<ALGO, MSG16, 24, 1024, 1>;
+  if (dcmax <= 32) return (const void*)bp_layered_kernel<ALGO, MSG16, 32, 1024, 1>;
   return nullptr;
 }
 
 template <int ALGO, int MSG16>
 static const void* lay_t(int dcmax, int maxt) {
-  if (maxt <= 384)
-    return ALGO == L_SPA ? lay_dc<ALGO, MSG16, 384, 1>(dcmax) : lay_dc<ALGO, MSG16, 384, 2>(dcmax);
-  return lay_dc<ALGO, MSG16, 1024, 1>(dcmax);
+  if (maxt > 384) return lay_wide<ALGO, MSG16>(dcmax);
+  if constexpr (ALGO == L_SPA) return lay_exact<ALGO, MSG16, 1>(dcmax);
+  else return lay_exact<ALGO, MSG16, 2>(dcmax);
 }
 
 int layered_dcmax_bucket(int max_dc) {
-  if (max_dc <= 8) return 8;
-  if (max_dc <= 12) return 12;
-  if (max_dc <= 16) return 16;
-  if (max_dc <= 24) return 24;
-  if (max_dc <= 32) return 32;
+  static const int buckets[] = {7, 9, 10, 11, 13, 14, 18, 19, 22, 26, 32};
+  for (int b : buckets)
+    if (max_dc <= b) return b;
   return -1;
 }
 
