@@ -257,10 +257,10 @@ class LdpcCode:
                                      ctypes.byref(nnz), ctypes.byref(lay)))
         self._n, self._m, self._k, self._nnz, self._layers = n.value, m.value, k.value, nnz.value, lay.value
 
-    def __del__(self):
+    def __del__(self, _destroy=_CODE_DESTROY):  # bound now: module globals may be gone at exit
         h = getattr(self, "_h", None)
         if h:
-            _CODE_DESTROY(h)
+            _destroy(h)
             self._h = None
 
     @classmethod
@@ -413,10 +413,10 @@ class LdpcDecoder:
         self._last_iterations = 0
         del keep
 
-    def __del__(self):
+    def __del__(self, _destroy=_DECODER_DESTROY):  # bound now: module globals may be gone at exit
         h = getattr(self, "_h", None)
         if h:
-            _DECODER_DESTROY(h)
+            _destroy(h)
             self._h = None
 
     def k(self):

@@ -61,10 +61,10 @@ class NmsTrainer:
         self.frame_counter = 0
         self.history = []
 
-    def __del__(self):
+    def __del__(self, _destroy=_TRAINER_DESTROY):  # bound now: module globals may be gone at exit
         h = getattr(self, "_h", None)
         if h:
-            _TRAINER_DESTROY(h)
+            _destroy(h)
             self._h = None
 
     @property
