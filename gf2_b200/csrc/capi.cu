@@ -359,6 +359,18 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   d->work_stride = c2v_bytes + (need_gapp ? ((long long)d->max_n * 4 + 255) / 256 * 256 : 0);
   d->kernel = layered ? layered_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax, threads)
                       : flood_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax);
+  if (layered && threads <= 384) {
+    // codes of different slot counts (a mixed batch): the kernel that runs each
+    // frame with its own code's exact slot count, where one exists
+    bool differ = false, dispatchable = true;
+    for (auto* c : d->codes) {
+      const int b = layered_dcmax_bucket(c->h->max_dc);
+      differ = differ || b != d->dcmax;
+      dispatchable = dispatchable && b > 0 && b <= 22;
+    }
+    const void* k = (differ && dispatchable) ? layered_kernel_ptr(o.algorithm, o.msg_dtype, 0, threads) : nullptr;
+    if (k) d->kernel = k;
+  }
   // Flooding min-sum / normalised-offset min-sum: the check-state kernel, with
   // the check states and posteriors in shared memory where they fit.
   const bool ms_family = o.algorithm == GF2C_ALGO_MINSUM || o.algorithm == GF2C_ALGO_NMS;

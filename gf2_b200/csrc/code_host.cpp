@@ -542,6 +542,7 @@ int upload_code(HostCode& c) {
     d.words_n = (int)((c.n + 63) / 64);
     d.words_m = (int)((c.m + 63) / 64);
     d.layered_ok = c.layered_ok;
+    d.lay_bucket = layered_dcmax_bucket(c.max_dc);
     d.max_nchk = c.max_nchk;
     int rc;
     if ((rc = dev_copy(c, c.cg, &d.cg))) return rc;

@@ -33,6 +33,7 @@ struct DevCode {
   int max_dc, max_dv;
   int words_k, words_n, words_m;   // ceil(x/64)
   int layered_ok;                  // CGs are layers usable by the layered schedule
+  int lay_bucket;                  // slot count of the layered kernel that fits this code exactly
   int max_nchk;                    // largest CG
   const int4* cg;                  // {chk_begin, nchk, dc, edge0}
   const uint32_t* cg_sync;         // layered: bit i = barrier after slot i (dup variables)

@@ -164,6 +164,172 @@ __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t,
   }
 }
 
+// Iterations of one frame with row groups of at most DCMAX slots; returns the
+// iteration count and whether the syndrome test passed at an early stop.
+template <int ALGO, int MSG16, int DCMAX>
+__device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const DevCode& C, float* app,
+                                                   typename MsgIO<MSG16>::T* __restrict__ c2v, const LayerSmem& S,
+                                                   int maxit, int& it, int& converged) {
+  typedef MsgIO<MSG16> IO;
+  const int tid = threadIdx.x, vgs = C.vgs, ncg = C.ncg;
+  const int4* __restrict__ cgp = C.cg;
+  const int4* __restrict__ spcg = C.sp_cg;
+  const uint32_t* __restrict__ cgs = C.cg_sync;
+  const int2* __restrict__ sdesc = C.sp_desc;
+  const uint32_t* __restrict__ absent = C.sp_absent;
+  const int2* __restrict__ vg = C.sp_vg;
+  const int* __restrict__ vg_chk = C.sp_ci;
+  it = 0;
+  converged = 0;
+  for (;;) {
+    const int tw = (a.nms_iters > 0) ? min(it, a.nms_iters - 1) : 0;
+    const bool first = (it == 0);
+    for (int g = 0; g < ncg; g++) {
+      const int4 G = cgp[g];
+      const uint32_t sync = cgs[g];
+      const bool act = tid < G.y;
+      const int d = G.z, nchk = G.y;
+      const int t = act ? tid : 0;
+      const int s0 = G.w + t;
+      const int2* __restrict__ sd = sdesc + spcg[g].w;
+      int vv[DCMAX];
+      float ap[DCMAX], o[DCMAX], w[DCMAX];
+      uint32_t real = 0, neg = 0, apneg = 0;
+      const uint32_t ab = (act && t == 0) ? __ldg(&absent[g]) : 0u;
+      if (ALGO == L_SPA_FAST && DCMAX <= 16 && act && sync == 0 && d == DCMAX && ab == 0) {
+        spa_fast_row<MSG16, DCMAX>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs);
+      } else if (act) {
+        // 1. indices, 2. all loads, 3. arithmetic
+#pragma unroll
+        for (int i = 0; i < DCMAX; i++)
+          vv[i] = (i < d && !((ab >> i) & 1u)) ? slot_u(__ldg(&sd[i]), t, nchk) : -1;
+#pragma unroll
+        for (int i = 0; i < DCMAX; i++) ap[i] = app[vv[i] < 0 ? 0 : vv[i]];
+        if (first) {
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) o[i] = 0.0f;
+        } else {
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) o[i] = ld_msg<MSG16>(c2v, (i < d) ? s0 + i * nchk : s0);
+        }
+#pragma unroll
+        for (int i = 0; i < DCMAX; i++) {
+          const bool r = vv[i] >= 0;
+          w[i] = __fsub_rn(ap[i], o[i]);  // v2c
+          real |= (uint32_t)r << i;
+          neg |= (uint32_t)(r && w[i] < 0.0f) << i;
+          apneg |= (uint32_t)(ap[i] < 0.0f) << i;
+        }
+        const int negp = __popc(neg) & 1;
+        const bool single = __popc(real) == 1;
+        if (ALGO == L_MS || ALGO == L_NMS) {
+          float m1 = __int_as_float(0x7f800000), m2 = m1;
+          int i1 = -1;
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) {
+            const float ax = ((real >> i) & 1u) ? fabsf(w[i]) : __int_as_float(0x7f800000);
+            if (ax < m1) {
+              m2 = m1;
+              m1 = ax;
+              i1 = i;
+            } else if (ax < m2) {
+              m2 = ax;
+            }
+          }
+          float mag1 = single ? 0.0f : m1, mag2 = single ? 0.0f : m2;
+          if (ALGO == L_NMS) {
+            const int lay = (a.nms_L == ncg) ? g : 0;
+            const float al = __ldg(&a.alpha[tw * a.nms_L + lay]);
+            const float be = __ldg(&a.beta[tw * a.nms_L + lay]);
+            const float d1 = __fsub_rn(mag1, be), d2 = __fsub_rn(mag2, be);
+            mag1 = __fmul_rn(al, d1 > 0.0f ? d1 : 0.0f);
+            mag2 = __fmul_rn(al, d2 > 0.0f ? d2 : 0.0f);
+          }
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) {
+            const float mag = (i == i1) ? mag2 : mag1;
+            w[i] = (negp ^ ((neg >> i) & 1u)) ? -mag : mag;
+          }
+        } else if (ALGO == L_SPA) {
+          float suf[DCMAX];
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) w[i] = ((real >> i) & 1u) ? tanh_half_f(w[i]) : 1.0f;
+          suf[DCMAX - 1] = 1.0f;
+#pragma unroll
+          for (int i = DCMAX - 2; i >= 0; i--) suf[i] = (i + 1 < d) ? __fmul_rn(w[i + 1], suf[i + 1]) : 1.0f;
+          float pre = 1.0f;
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) {
+            float p = __fmul_rn(pre, suf[i]);
+            p = p > GF2C_SPA_PMAX ? GF2C_SPA_PMAX : (p < -GF2C_SPA_PMAX ? -GF2C_SPA_PMAX : p);
+            const float out = single ? 0.0f : two_atanh_f(p);
+            if (i < d) pre = (i == 0) ? w[0] : __fmul_rn(pre, w[i]);
+            w[i] = out;
+          }
+        } else {  // fast sum-product; ap[] keeps v2c for the APP update
+          float N = 1.0f, Dp = 1.0f;
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) {
+            const float x = w[i];
+            ap[i] = x;
+            const float e = ((real >> i) & 1u) ? ex2_approx(fabsf(x) * -1.4426950408889634f) : 0.0f;
+            w[i] = e;
+            N *= fmaxf(1.0f - e, 5.9604645e-08f);
+            Dp = __fmaf_rn(Dp, e, Dp);
+          }
+#pragma unroll
+          for (int i = 0; i < DCMAX; i++) {
+            const float ni = fmaxf(1.0f - w[i], 5.9604645e-08f), di = 1.0f + w[i];
+            const float num = __fmaf_rn(Dp, ni, N * di);
+            const float den = fmaxf(__fmaf_rn(Dp, ni, -N * di), num * 5.9604645e-08f);
+            float mag = 0.69314718055994531f * lg2_approx(num * rcp_approx(den));
+            mag = single ? 0.0f : fminf(mag, 16.635532f);
+            w[i] = (negp ^ ((neg >> i) & 1u)) ? -mag : mag;
+          }
+        }
+        // message stores; APP update for row groups without repeated variables
+#pragma unroll
+        for (int i = 0; i < DCMAX; i++) {
+          if ((real >> i) & 1u) {
+            const float out = IO::rt(w[i]);
+            st_msg<MSG16>(c2v, s0 + i * nchk, out);
+            if (ALGO == L_SPA_FAST) {
+              if (sync == 0) app_put(app, vv[i], (apneg >> i) & 1u, ap[i] + out, S, vg, vg_chk, vgs);
+              else w[i] = out - o[i];
+            } else {
+              w[i] = __fsub_rn(out, o[i]);  // delta
+              if (sync == 0) app_put(app, vv[i], (apneg >> i) & 1u, __fadd_rn(ap[i], w[i]), S, vg, vg_chk, vgs);
+            }
+          }
+        }
+      }
+      if (sync != 0) {
+        __syncthreads();  // all pre-layer APP reads done
+#pragma unroll
+        for (int i = 0; i < DCMAX; i++) {
+          if (i < d) {
+            if (act && ((real >> i) & 1u)) {
+              const int v = vv[i];
+              const float ov = app[v];
+              app_put(app, v, ov < 0.0f, __fadd_rn(ov, w[i]), S, vg, vg_chk, vgs);
+            }
+            if ((sync >> i) & 1u) __syncthreads();
+          }
+        }
+      }
+      __syncthreads();
+    }
+    ++it;
+    const int unsat = *S.unsat;
+    if (a.early_stop && unsat == 0) {
+      converged = 1;
+      break;
+    }
+    if (it >= maxit) break;
+    __syncthreads();  // s_unsat read by all before the next iteration's updates
+  }
+}
+
 template <int ALGO, int MSG16, int DCMAX, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs a) {
   typedef typename MsgIO<MSG16>::T MsgT;
@@ -200,15 +366,11 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
     }
     if (tid == 0) C = a.codes[cid];
     __syncthreads();
-    const int n = C.n, m = C.m, vgs = C.vgs, ncg = C.ncg;
-    const int4* __restrict__ cgp = C.cg;
+    const int n = C.n, m = C.m;
     const int4* __restrict__ spcg = C.sp_cg;
-    const uint32_t* __restrict__ cgs = C.cg_sync;
     const int2* __restrict__ sdesc = C.sp_desc;
     const uint32_t* __restrict__ absent = C.sp_absent;
     const int* __restrict__ u2v = C.sp_u2v;
-    const int2* __restrict__ vg = C.sp_vg;
-    const int* __restrict__ vg_chk = C.sp_ci;
     const float* __restrict__ llr = a.llr + (a.llr_off ? a.llr_off[f] : f * (long long)n);
     const int maxit = a.max_iter_arr ? a.max_iter_arr[f] : a.max_iter;
     float* app = (n <= a.smem_app_floats) ? smem_app : gapp;
@@ -266,152 +428,20 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
     __syncthreads();
 
     int it = 0, converged = 0;
-    for (;;) {
-      const int tw = (a.nms_iters > 0) ? min(it, a.nms_iters - 1) : 0;
-      const bool first = (it == 0);
-      for (int g = 0; g < ncg; g++) {
-        const int4 G = cgp[g];
-        const uint32_t sync = cgs[g];
-        const bool act = tid < G.y;
-        const int d = G.z, nchk = G.y;
-        const int t = act ? tid : 0;
-        const int s0 = G.w + t;
-        const int2* __restrict__ sd = sdesc + spcg[g].w;
-        int vv[DCMAX];
-        float ap[DCMAX], o[DCMAX], w[DCMAX];
-        uint32_t real = 0, neg = 0, apneg = 0;
-        const uint32_t ab = (act && t == 0) ? __ldg(&absent[g]) : 0u;
-        if (ALGO == L_SPA_FAST && DCMAX <= 16 && act && sync == 0 && d == DCMAX && ab == 0) {
-          spa_fast_row<MSG16, DCMAX>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs);
-        } else if (act) {
-          // 1. indices, 2. all loads, 3. arithmetic
-#pragma unroll
-          for (int i = 0; i < DCMAX; i++)
-            vv[i] = (i < d && !((ab >> i) & 1u)) ? slot_u(__ldg(&sd[i]), t, nchk) : -1;
-#pragma unroll
-          for (int i = 0; i < DCMAX; i++) ap[i] = app[vv[i] < 0 ? 0 : vv[i]];
-          if (first) {
-#pragma unroll
-            for (int i = 0; i < DCMAX; i++) o[i] = 0.0f;
-          } else {
-#pragma unroll
-            for (int i = 0; i < DCMAX; i++) o[i] = ld_msg<MSG16>(c2v, (i < d) ? s0 + i * nchk : s0);
-          }
-#pragma unroll
-          for (int i = 0; i < DCMAX; i++) {
-            const bool r = vv[i] >= 0;
-            w[i] = __fsub_rn(ap[i], o[i]);  // v2c
-            real |= (uint32_t)r << i;
-            neg |= (uint32_t)(r && w[i] < 0.0f) << i;
-            apneg |= (uint32_t)(ap[i] < 0.0f) << i;
-          }
-          const int negp = __popc(neg) & 1;
-          const bool single = __popc(real) == 1;
-          if (ALGO == L_MS || ALGO == L_NMS) {
-            float m1 = __int_as_float(0x7f800000), m2 = m1;
-            int i1 = -1;
-#pragma unroll
-            for (int i = 0; i < DCMAX; i++) {
-              const float ax = ((real >> i) & 1u) ? fabsf(w[i]) : __int_as_float(0x7f800000);
-              if (ax < m1) {
-                m2 = m1;
-                m1 = ax;
-                i1 = i;
-              } else if (ax < m2) {
-                m2 = ax;
-              }
-            }
-            float mag1 = single ? 0.0f : m1, mag2 = single ? 0.0f : m2;
-            if (ALGO == L_NMS) {
-              const int lay = (a.nms_L == ncg) ? g : 0;
-              const float al = __ldg(&a.alpha[tw * a.nms_L + lay]);
-              const float be = __ldg(&a.beta[tw * a.nms_L + lay]);
-              const float d1 = __fsub_rn(mag1, be), d2 = __fsub_rn(mag2, be);
-              mag1 = __fmul_rn(al, d1 > 0.0f ? d1 : 0.0f);
-              mag2 = __fmul_rn(al, d2 > 0.0f ? d2 : 0.0f);
-            }
-#pragma unroll
-            for (int i = 0; i < DCMAX; i++) {
-              const float mag = (i == i1) ? mag2 : mag1;
-              w[i] = (negp ^ ((neg >> i) & 1u)) ? -mag : mag;
-            }
-          } else if (ALGO == L_SPA) {
-            float suf[DCMAX];
-#pragma unroll
-            for (int i = 0; i < DCMAX; i++) w[i] = ((real >> i) & 1u) ? tanh_half_f(w[i]) : 1.0f;
-            suf[DCMAX - 1] = 1.0f;
-#pragma unroll
-            for (int i = DCMAX - 2; i >= 0; i--) suf[i] = (i + 1 < d) ? __fmul_rn(w[i + 1], suf[i + 1]) : 1.0f;
-            float pre = 1.0f;
-#pragma unroll
-            for (int i = 0; i < DCMAX; i++) {
-              float p = __fmul_rn(pre, suf[i]);
-              p = p > GF2C_SPA_PMAX ? GF2C_SPA_PMAX : (p < -GF2C_SPA_PMAX ? -GF2C_SPA_PMAX : p);
-              const float out = single ? 0.0f : two_atanh_f(p);
-              if (i < d) pre = (i == 0) ? w[0] : __fmul_rn(pre, w[i]);
-              w[i] = out;
-            }
-          } else {  // fast sum-product; ap[] keeps v2c for the APP update
-            float N = 1.0f, Dp = 1.0f;
-#pragma unroll
-            for (int i = 0; i < DCMAX; i++) {
-              const float x = w[i];
-              ap[i] = x;
-              const float e = ((real >> i) & 1u) ? ex2_approx(fabsf(x) * -1.4426950408889634f) : 0.0f;
-              w[i] = e;
-              N *= fmaxf(1.0f - e, 5.9604645e-08f);
-              Dp = __fmaf_rn(Dp, e, Dp);
-            }
-#pragma unroll
-            for (int i = 0; i < DCMAX; i++) {
-              const float ni = fmaxf(1.0f - w[i], 5.9604645e-08f), di = 1.0f + w[i];
-              const float num = __fmaf_rn(Dp, ni, N * di);
-              const float den = fmaxf(__fmaf_rn(Dp, ni, -N * di), num * 5.9604645e-08f);
-              float mag = 0.69314718055994531f * lg2_approx(num * rcp_approx(den));
-              mag = single ? 0.0f : fminf(mag, 16.635532f);
-              w[i] = (negp ^ ((neg >> i) & 1u)) ? -mag : mag;
-            }
-          }
-          // message stores; APP update for row groups without repeated variables
-#pragma unroll
-          for (int i = 0; i < DCMAX; i++) {
-            if ((real >> i) & 1u) {
-              const float out = IO::rt(w[i]);
-              st_msg<MSG16>(c2v, s0 + i * nchk, out);
-              if (ALGO == L_SPA_FAST) {
-                if (sync == 0) app_put(app, vv[i], (apneg >> i) & 1u, ap[i] + out, S, vg, vg_chk, vgs);
-                else w[i] = out - o[i];
-              } else {
-                w[i] = __fsub_rn(out, o[i]);  // delta
-                if (sync == 0) app_put(app, vv[i], (apneg >> i) & 1u, __fadd_rn(ap[i], w[i]), S, vg, vg_chk, vgs);
-              }
-            }
-          }
-        }
-        if (sync != 0) {
-          __syncthreads();  // all pre-layer APP reads done
-#pragma unroll
-          for (int i = 0; i < DCMAX; i++) {
-            if (i < d) {
-              if (act && ((real >> i) & 1u)) {
-                const int v = vv[i];
-                const float ov = app[v];
-                app_put(app, v, ov < 0.0f, __fadd_rn(ov, w[i]), S, vg, vg_chk, vgs);
-              }
-              if ((sync >> i) & 1u) __syncthreads();
-            }
-          }
-        }
-        __syncthreads();
+    if constexpr (DCMAX > 0) {
+      layered_iterations<ALGO, MSG16, DCMAX>(a, C, app, c2v, S, maxit, it, converged);
+    } else {  // mixed batch: the exact slot count of this frame's code
+      switch (C.lay_bucket) {
+        case 7: layered_iterations<ALGO, MSG16, 7>(a, C, app, c2v, S, maxit, it, converged); break;
+        case 9: layered_iterations<ALGO, MSG16, 9>(a, C, app, c2v, S, maxit, it, converged); break;
+        case 10: layered_iterations<ALGO, MSG16, 10>(a, C, app, c2v, S, maxit, it, converged); break;
+        case 11: layered_iterations<ALGO, MSG16, 11>(a, C, app, c2v, S, maxit, it, converged); break;
+        case 13: layered_iterations<ALGO, MSG16, 13>(a, C, app, c2v, S, maxit, it, converged); break;
+        case 14: layered_iterations<ALGO, MSG16, 14>(a, C, app, c2v, S, maxit, it, converged); break;
+        case 18: layered_iterations<ALGO, MSG16, 18>(a, C, app, c2v, S, maxit, it, converged); break;
+        case 19: layered_iterations<ALGO, MSG16, 19>(a, C, app, c2v, S, maxit, it, converged); break;
+        default: layered_iterations<ALGO, MSG16, 22>(a, C, app, c2v, S, maxit, it, converged); break;
       }
-      ++it;
-      const int unsat = s_unsat;
-      if (a.early_stop && unsat == 0) {
-        converged = 1;
-        break;
-      }
-      if (it >= maxit) break;
-      __syncthreads();  // s_unsat read by all before the next iteration's updates
     }
     if (!converged) converged = (s_unsat == 0);
 
@@ -453,6 +483,9 @@ static const void* lay_exact(int dcmax) {
     case 22: return (const void*)bp_layered_kernel<ALGO, MSG16, 22, 384, MINB>;
     case 26: return (const void*)bp_layered_kernel<ALGO, MSG16, 26, 384, MINB>;
     case 32: return (const void*)bp_layered_kernel<ALGO, MSG16, 32, 384, MINB>;
+    case 0:  // mixed batches: each frame runs the iterations of its code's exact slot count
+      if constexpr (ALGO == L_SPA_FAST) return (const void*)bp_layered_kernel<ALGO, MSG16, 0, 384, MINB>;
+      return nullptr;
   }
   return nullptr;
 }

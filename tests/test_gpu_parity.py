@@ -275,6 +275,37 @@ def test_mixed_batch_matches_single(gpu, oracle):
         assert (r["msg"][mo[f]:mo[f] + w] == single["msg"][0]).all()
 
 
+def test_mixed_layered_batch_matches_single(gpu, oracle):
+    """A mixed layered batch runs every frame with its own code's slot count:
+    the results equal per-code decoders with the same options."""
+    idxs = [6, 1, 11, 9]  # short 1/2 (7 slots), normal 3/5 (11), short 5/6 (19), short 3/4 (13)
+    codes = [dvb(i) for i in idxs]
+    kw = dict(algorithm=g.ALGO_SPA_FAST, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16)
+    dec = g.LdpcDecoder(codes[0], codes=codes, **kw)
+    F = 16
+    cid = np.array([f % len(codes) for f in range(F)], np.int32)
+    mit = np.array([5 + 3 * (f % 7) for f in range(F)], np.int32)
+    llrs, lo, mo = [], [], []
+    off = moff = 0
+    for f in range(F):
+        i = idxs[cid[f]]
+        oc = oracle.Code.dvbt2(i // 6, i % 6)
+        _, _, l = oc.channel(21, f, 1, {6: 1.2, 1: 1.1, 11: 3.2, 9: 2.4}[i])
+        llrs.append(l[0])
+        lo.append(off)
+        mo.append(moff)
+        off += oc.n
+        moff += g.words(oc.k)
+    r = dec.decode_mixed_arrays(np.concatenate(llrs), lo, cid, mit, mo)
+    for f in range(F):
+        c = codes[cid[f]]
+        single = g.LdpcDecoder(c, **kw).decode_arrays(llrs[f][None, :], int(mit[f]))
+        assert r["iters"][f] == single["iters"][0]
+        assert r["conv"][f] == single["conv"][0]
+        w = g.words(c.k())
+        assert (r["msg"][mo[f]:mo[f] + w] == single["msg"][0]).all()
+
+
 def test_mixed_batch_graph_replay(gpu):
     import torch
     codes = [g.LdpcCode.dvb_t2_short(0), g.LdpcCode.dvb_t2_short(4)]
