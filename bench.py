@@ -27,6 +27,10 @@ Workloads (one "step" = one decode of the whole batch):
                 timing), 10 flooding iterations, FP16 messages, early stop; frames
                 still failing the syndrome are re-decoded by 50-iteration
                 sum-product; frame f at Eb/N0 = 2.6 + 0.1 (f mod 9) dB.
+  bch           DVB-T2 normal 3/5 outer BCH code (n=38880, k=38688, t=12),
+                65536 packed words, frame f with f mod 13 random bit errors;
+                syndromes, Berlekamp-Massey and Chien search on the device
+                (metric: BCH decoded info Gbit/s).
 
 The LLR input of every workload is larger than L2 (no flush needed).
 `--impl reference` times the reference decoder's CPU restatement (flooding
@@ -67,7 +71,10 @@ SINGLE = {
                   desc="dvbt2-short-1/2 flooding min-sum fp32 (reference decoder), 256 frames, "
                        "Eb/N0 1.0 dB, max 50 it"),
 }
-WORKLOADS = sorted(list(SINGLE) + ["c3", "c5"])
+WORKLOADS = sorted(list(SINGLE) + ["c3", "c5", "bch"])
+BCH_METRIC = "BCH decoded info Gbit/s on 1 B200 (DVB-T2 outer code, hard decision)"
+BCH_DESC = ("dvbt2-normal-3/5 outer BCH (n=38880, k=38688, t=12) hard-decision decode, 65536 frames, "
+            "frame f carries f mod 13 random bit errors (0..t, every frame corrected)")
 
 
 def parse():
@@ -475,11 +482,139 @@ def shannon_limit(rate):
     return (lo + hi) / 2
 
 
+def bch_frames(frames, seed):
+    """Seeded BCH test words of the bch workload as one bit per byte (CPU):
+    random messages, frame f with f mod 13 flipped bits at distinct positions."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    n, k, t = 38880, 38688, 12
+    msg = rng.integers(0, 2, (frames, k), dtype=np.uint8)
+    errs = [(f, rng.choice(n, size=f % (t + 1), replace=False)) for f in range(frames)]
+    return msg, errs
+
+
+class BchBatch:
+    """DVB-T2 normal 3/5 outer BCH decode of a device batch of packed words."""
+
+    def __init__(self, dev, rank, frames):
+        import numpy as np
+        import torch
+
+        import gf2_b200 as g
+        self.g = g
+        self.frames = frames or 65536
+        self.code = g.BchCode.dvb_t2(0, 1)
+        n, k, t = self.code.n(), self.code.k(), self.code.t()
+        F, wk, wn = self.frames, g.words(k), g.words(n)
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(1000 + rank)
+        m = torch.randint(-2 ** 31, 2 ** 31, (F, 2 * wk), dtype=torch.int32, device=dev, generator=gen)
+        self.msg_words = m.view(torch.int64)
+        if k & 63:
+            self.msg_words[:, -1] &= (1 << (k & 63)) - 1
+        cw = g.BchEncoder(self.code).encode_words(self.msg_words)
+        # f mod (t+1) errors per frame at distinct positions, XORed in on the host
+        rng = np.random.default_rng(2000 + rank)
+        h = cw.cpu().numpy().view(np.uint64)
+        fi, wi, bi = [], [], []
+        for f in range(F):
+            pos = rng.choice(n, size=f % (t + 1), replace=False)
+            fi.append(np.full(len(pos), f))
+            wi.append(pos >> 6)
+            bi.append(pos & 63)
+        fi, wi, bi = np.concatenate(fi), np.concatenate(wi), np.concatenate(bi)
+        np.bitwise_xor.at(h, (fi, wi), np.left_shift(np.uint64(1), bi.astype(np.uint64)))
+        self.expect_flips = np.array([f % (t + 1) for f in range(F)], np.int32)
+        self.cw = torch.from_numpy(h.view(np.int64)).to(dev)
+        self.dec = g.BchDecoder(self.code)
+        self.out = None
+        self.desc = BCH_DESC
+        self.dtype = "u16"
+        self.stream = torch.cuda.current_stream(dev)
+
+    def step(self):
+        self.out = self.dec.decode_words(self.cw, stream=self.stream)
+
+    def launches(self):
+        return 1
+
+    def bits_per_step(self):
+        return self.frames * self.code.k()
+
+    def stats(self):
+        fl = self.out["corrected"].cpu().numpy()
+        ok = bool((fl == self.expect_flips).all()) and bool(torch_equal(self.out["msg"], self.msg_words))
+        g, c = self.g, self.code
+        per = 8 * g.words(c.n()) + 8 * g.words(c.k()) + 4
+        return self.frames * per, {"corrected_mean": float(fl.mean()), "all_frames_recovered": ok,
+                                   "errors_per_frame": "f mod 13"}
+
+    def host_step_factory(self):
+        """The public C-ABI host path: pinned packed words in, messages out."""
+        import ctypes
+
+        import torch
+
+        from gf2_b200 import _capi as C
+        g, c, F = self.g, self.code, self.frames
+        h_cw = torch.empty_like(self.cw, device="cpu").pin_memory()
+        h_cw.copy_(self.cw.cpu())
+        h_msg = torch.empty((F, g.words(c.k())), dtype=torch.int64, pin_memory=True)
+        h_fl = torch.empty(F, dtype=torch.int32, pin_memory=True)
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())
+
+        def host_step():
+            C.check(C.lib.gf2c_bch_decode_batch(c.handle, vp(h_cw), F, vp(h_msg), vp(h_fl), None, C.MEM_HOST,
+                                                None))
+        return host_step, F * g.words(c.n()) * 8, F * (g.words(c.k()) * 8 + 4)
+
+
+def torch_equal(a, b):
+    import torch
+    return torch.equal(a, b)
+
+
+def run_cpu_bch(steps, warmup, cores=None, frames=None):
+    """The BCH oracle (restatement of BchDecoder::decode) over a sample of the
+    bch workload's words, chunks decoded concurrently on all host threads."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+
+    from oracle import pyoracle
+    pyoracle.build()
+    cores = cores or os.cpu_count() or 1
+    b = pyoracle.Bch(0, 1)
+    S = frames or 13 * max(1, round(100 * cores / 13))
+    msg, errs = bch_frames(S, 7)
+    cw = b.encode(msg)
+    for f, pos in errs:
+        cw[f, pos] ^= 1
+    chunks = np.array_split(np.arange(S), cores)
+    times = []
+    for s in range(warmup + steps):
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(cores) as ex:
+            outs = list(ex.map(lambda ix: b.decode(cw[ix]), [c for c in chunks if len(c)]))
+        dt = time.perf_counter() - t0
+        if s >= warmup:
+            times.append(dt)
+    dm = np.concatenate([o[0] for o in outs])
+    assert (dm == msg).all()
+    tot = sum(times)
+    gbps = S * b.k * len(times) / tot / 1e9
+    sample = (f"{S} words of the bch workload's code (f mod 13 errors), BCH oracle decode on {cores} threads, "
+              f"{len(times)} timed passes of {tot / len(times):.2f} s")
+    return gbps, dict(cores=cores, sample=sample, frames=S)
+
+
 def make_workload(name, dev, rank, frames):
     if name in SINGLE:
         return SingleCode(name, dev, rank, frames)
     if name == "c3":
         return Mixed(dev, rank, frames)
+    if name == "bch":
+        return BchBatch(dev, rank, frames)
     return LearnedScale(dev, rank, frames)
 
 
@@ -492,12 +627,17 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        gbps, info = run_cpu_reference(args.workload, 1, args.steps, args.warmup)
-        desc = SINGLE[args.workload]["desc"] if args.workload in SINGLE else args.workload
-        line = {"metric": METRIC, "value": gbps, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        if args.workload == "bch":
+            gbps, info = run_cpu_bch(args.steps, args.warmup)
+            desc, decoder, metric = BCH_DESC, "reference BchDecoder::decode (CPU restatement)", BCH_METRIC
+        else:
+            gbps, info = run_cpu_reference(args.workload, 1, args.steps, args.warmup)
+            desc = SINGLE[args.workload]["desc"] if args.workload in SINGLE else args.workload
+            decoder, metric = "reference flooding min-sum (CPU restatement)", METRIC
+        line = {"metric": metric, "value": gbps, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox AWGN frames)",
-                "config": {"workload": desc, "decoder": "reference flooding min-sum (CPU restatement)"},
+                "config": {"workload": desc, "decoder": decoder},
                 "cpu_baseline": {"value": gbps, "unit": UNIT, "cores": info["cores"], "kind": "port",
                                  "sample": info["sample"]},
                 "e2e": {"value": gbps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -575,14 +715,18 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        gbps, info = run_cpu_reference(args.workload, 1, 1, 0)
+        if args.workload == "bch":
+            gbps, info = run_cpu_bch(1, 0)
+        else:
+            gbps, info = run_cpu_reference(args.workload, 1, 1, 0)
         cpu = {"value": gbps, "unit": UNIT, "cores": info["cores"], "kind": "port", "sample": info["sample"]}
 
     if rank == 0:
         config = {"workload": wl.desc, "frames_per_gpu": getattr(wl, "frames", None),
                   "l2": "inputs larger than L2 (no flush)",
                   "parallelism": f"replicas x{world} (frames sharded by index, no data-path collective)"}
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        line = {"metric": BCH_METRIC if args.workload == "bch" else METRIC, "value": value, "unit": UNIT,
+                "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype,
                 "data": "synthetic (seeded Philox AWGN frames, BPSK, encoder output)", "config": config,

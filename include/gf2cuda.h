@@ -234,6 +234,34 @@ int gf2c_count_errors(const uint64_t* ref_bits, const uint64_t* test_bits, int64
 int gf2c_adam_step(float* params, const float* grads, float* m, float* v, int64_t count, float lr,
                    float beta1, float beta2, float eps, int32_t step, float lo, float hi, void* stream);
 
+/* ---- DVB-T2 outer BCH code (the step after LDPC decoding) ----
+ * A BCH code handle holds one of the 12 DVB-T2 outer codes: n = k_ldpc of the
+ * matching LDPC code, k = Kbch, t = 12 (10 for normal 2/3 and 5/6), GF(2^14)
+ * for short and GF(2^16) for normal frames.  Codewords are [message | parity]
+ * with bit i the coefficient of degree n-1-i (the reference's convention), in
+ * the packed BitVec layout. */
+typedef struct gf2c_bch gf2c_bch;
+/* BchCode::dvb_t2 (crates/gf2-coding/src/bch/dvb_t2/mod.rs:62-78,
+ * params.rs:56-85, generators.rs:14-62); frame_size / rate as for the LDPC codes. */
+int gf2c_bch_create_dvbt2(int32_t frame_size, int32_t rate, gf2c_bch** out);
+int gf2c_bch_destroy(gf2c_bch* bch);
+/* BchCode::{n, k, t} (bch/core.rs:235-247) and the field degree m. */
+int gf2c_bch_dims(const gf2c_bch* bch, int64_t* n, int64_t* k, int32_t* t, int32_t* field_m);
+/* BchCode::generator (bch/core.rs:255): n-k+1 binary coefficients, x^d at [d]. */
+int gf2c_bch_generator(const gf2c_bch* bch, uint8_t* coeffs);
+/* BchEncoder::{encode, encode_batch} (bch/core.rs:396-480): frames x ceil(k/64)
+ * message words in, frames x ceil(n/64) codeword words out. */
+int gf2c_bch_encode_batch(gf2c_bch* bch, const uint64_t* msg_bits, int64_t frames, uint64_t* cw_bits,
+                          int32_t mem, void* stream);
+/* BchDecoder::{decode, decode_batch} (bch/core.rs:542-665): frames x ceil(n/64)
+ * codeword words in, frames x ceil(k/64) message words out, bit-identical to
+ * the reference (syndromes, Berlekamp-Massey, Chien search, no check of the
+ * root count).  corrected (nullable): bits flipped per frame (the number of
+ * roots found); syndromes (nullable): frames x 2t elements S_1..S_2t of
+ * BchDecoder::compute_syndromes (bch/core.rs:562-617). */
+int gf2c_bch_decode_batch(gf2c_bch* bch, const uint64_t* cw_bits, int64_t frames, uint64_t* msg_bits,
+                          int32_t* corrected, uint16_t* syndromes, int32_t mem, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

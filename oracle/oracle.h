@@ -113,6 +113,22 @@ double or_nms_loss_grad(const or_code* c, const float* llr, const uint8_t* cw,
 uint16_t or_f32_to_f16(float x);
 float or_f16_to_f32(uint16_t h);
 
+/* ---- DVB-T2 outer BCH code (bch.cpp) ----
+ * Codewords are [message (k) | parity (n-k)], bit i at polynomial degree n-1-i.
+ * out5 = {n, k, t, field degree m, generator degree}.  Syndromes S_1..S_2t as
+ * GF(2^m) elements (polynomial basis of the DVB-T2 primitive polynomial).
+ * or_bch_decode writes the k message bits and, per frame, the number of bits
+ * it flipped (the Chien-search roots). */
+typedef struct or_bch or_bch;
+or_bch* or_bch_dvbt2(int frame, int rate);
+void or_bch_free(or_bch* b);
+void or_bch_dims(const or_bch* b, int64_t* out5);
+void or_bch_generator(const or_bch* b, uint8_t* coeffs /* degree + 1, x^d at [d] */);
+void or_bch_encode(const or_bch* b, const uint8_t* msg, int64_t frames, uint8_t* cw);
+void or_bch_syndromes(const or_bch* b, const uint8_t* cw, int64_t frames, uint16_t* synd);
+int or_bch_berlekamp_massey(const or_bch* b, const uint16_t* synd, uint16_t* lambda /* 2t+1 */);
+void or_bch_decode(const or_bch* b, const uint8_t* cw, int64_t frames, uint8_t* msg, int32_t* nflips);
+
 #ifdef __cplusplus
 }
 #endif

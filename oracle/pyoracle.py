@@ -73,6 +73,17 @@ def lib():
         L.or_f32_to_f16.argtypes = [ctypes.c_float]
         L.or_f16_to_f32.restype = ctypes.c_float
         L.or_f16_to_f32.argtypes = [ctypes.c_uint16]
+        _u16p = ctypes.POINTER(ctypes.c_uint16)
+        L.or_bch_dvbt2.restype = ctypes.c_void_p
+        L.or_bch_dvbt2.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.or_bch_free.argtypes = [ctypes.c_void_p]
+        L.or_bch_dims.argtypes = [ctypes.c_void_p, _i64p]
+        L.or_bch_generator.argtypes = [ctypes.c_void_p, _u8p]
+        L.or_bch_encode.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_int64, _u8p]
+        L.or_bch_syndromes.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_int64, _u16p]
+        L.or_bch_berlekamp_massey.restype = ctypes.c_int
+        L.or_bch_berlekamp_massey.argtypes = [ctypes.c_void_p, _u16p, _u16p]
+        L.or_bch_decode.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_int64, _u8p, _i32p]
         _LIB = L
     return _LIB
 
@@ -249,3 +260,53 @@ def shannon_limit(rate):
 
 def f32_to_f16_bits(x):
     return lib().or_f32_to_f16(x)
+
+
+class Bch:
+    """DVB-T2 outer BCH code (bch.cpp): BchCode::dvb_t2, encode, syndromes,
+    Berlekamp-Massey, decode (bits one per byte)."""
+
+    def __init__(self, frame, rate):
+        self.h = lib().or_bch_dvbt2(frame, rate)
+        if not self.h:
+            raise OracleError("bad DVB-T2 BCH frame / rate")
+        d = np.zeros(5, np.int64)
+        lib().or_bch_dims(self.h, _p(d, _i64p))
+        self.n, self.k, self.t, self.field_m, self.gen_degree = (int(x) for x in d)
+
+    def __del__(self):
+        try:
+            lib().or_bch_free(self.h)
+        except Exception:
+            pass
+
+    def generator(self):
+        g = np.zeros(self.gen_degree + 1, np.uint8)
+        lib().or_bch_generator(self.h, _p(g, _u8p))
+        return g
+
+    def encode(self, msg):
+        m = np.ascontiguousarray(msg, np.uint8).reshape(-1, self.k)
+        cw = np.zeros((m.shape[0], self.n), np.uint8)
+        lib().or_bch_encode(self.h, _p(m, _u8p), m.shape[0], _p(cw, _u8p))
+        return cw
+
+    def syndromes(self, cw):
+        c = np.ascontiguousarray(cw, np.uint8).reshape(-1, self.n)
+        s = np.zeros((c.shape[0], 2 * self.t), np.uint16)
+        lib().or_bch_syndromes(self.h, _p(c, _u8p), c.shape[0], _p(s, ctypes.POINTER(ctypes.c_uint16)))
+        return s
+
+    def berlekamp_massey(self, synd):
+        s = np.ascontiguousarray(synd, np.uint16)
+        lam = np.zeros(2 * self.t + 1, np.uint16)
+        deg = lib().or_bch_berlekamp_massey(self.h, _p(s, ctypes.POINTER(ctypes.c_uint16)),
+                                            _p(lam, ctypes.POINTER(ctypes.c_uint16)))
+        return lam[:deg + 1]
+
+    def decode(self, cw):
+        c = np.ascontiguousarray(cw, np.uint8).reshape(-1, self.n)
+        msg = np.zeros((c.shape[0], self.k), np.uint8)
+        flips = np.zeros(c.shape[0], np.int32)
+        lib().or_bch_decode(self.h, _p(c, _u8p), c.shape[0], _p(msg, _u8p), _p(flips, _i32p))
+        return msg, flips
