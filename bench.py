@@ -536,7 +536,7 @@ class BchBatch:
         self.out = self.dec.decode_words(self.cw, stream=self.stream)
 
     def launches(self):
-        return 1
+        return 2  # syndrome / Berlekamp-Massey kernel + Chien kernel
 
     def bits_per_step(self):
         return self.frames * self.code.k()

@@ -11,20 +11,31 @@
 //                                            bch/core.rs:562-818
 // alpha = x in GF(2^m) modulo the DVB-T2 primitive polynomial.
 //
-// GPU layout: one warp per frame, frames from a grid-stride loop.
-//  * Encoder: parity = XOR over the set message bits i of the remainder row
-//    x^(r + k-1-i) mod g (precomputed per code, r bits, L2-resident); lanes
-//    split the message bits and XOR-reduce their rows.
-//  * Syndromes: S_j = alpha^(j(n-1)) * sum_i b_i beta^i with beta = alpha^-j.
-//    Per 64-bit word of the codeword the inner sum is 8 lookups in per-(j,
-//    byte position) tables of 256 entries (shared memory, odd j only), then
-//    one multiplication by beta^(64 w); even syndromes are squares (binary
-//    received word: r(alpha^2j) = r(alpha^j)^2).
-//  * Frames with a nonzero syndrome: lane 0 runs the reference's
-//    Berlekamp-Massey step for step, then the lanes evaluate the locator at
-//    alpha^-i for their positions i (Chien search) and flip the bits of the
-//    roots that fall in the message.
-// Field multiplications use log / antilog tables (global memory, L1-cached).
+// GPU layout: one warp per frame.
+//  * Odd syndromes S_j, j = 2s+1 < 2t (shared by encoder and decoder):
+//    S_j = alpha^(j(n-1)) sum_i b_i beta^i, beta = alpha^-j.  Lane l takes the
+//    64-bit words w = l + 32u (coalesced) and runs Horner over u from the top,
+//    acc <- acc * beta^2048 + q_w, where q_w = sum over the word's 8 bytes of a
+//    per-(byte position, value) table entry that packs four syndromes in 8
+//    bytes; the multiply by the constant beta^2048 is two byte lookups.  The
+//    lane's sum is scaled by alpha^(j(n-1-64l)) and XOR-reduced over the warp.
+//    All tables live in shared memory.  Even syndromes are squares:
+//    S_(2^a o) = S_o^(2^a) for a binary received word.
+//  * Encoder: the odd syndromes of [message | 0] fix the parity, because the
+//    map from the r parity bits to the r = t m odd-syndrome bits is invertible
+//    (g is the product of the minimal polynomials of alpha^j, j odd < 2t).
+//    parity = A s with A the inverse of that GF(2) matrix (host-built); it
+//    equals x^r m(x) mod g, the unique systematic parity.
+//  * Decoder, kernel 1: syndromes, the message copy, and the reference's
+//    Berlekamp-Massey step for step with lane i holding coefficient i of the
+//    locator and of the correction polynomial (the discrepancy is a warp XOR
+//    reduction).  It stores the locator as logarithms per frame.
+//  * Decoder, kernel 2 (Chien search): the antilog table of the field in
+//    shared memory; lane l evaluates positions i = l + 32s with the terms'
+//    exponents in registers (locator degrees 1..12 unrolled); a root i flips
+//    bit n-1-i when it lies in the message.  A frame stops once it has found
+//    deg(lambda) roots (a polynomial has no more), which returns the same
+//    roots as the full search.  Frames are taken from an atomic counter.
 #include <algorithm>
 #include <cstring>
 #include <memory>
@@ -34,206 +45,360 @@
 
 namespace gf2c {
 
-static constexpr int kBchMaxT = 12;
-static constexpr int kBchWarps = 8;  // frames per CTA at a time
+static constexpr int kBchWarps = 8;          // warps per CTA in the syndrome kernels
+static constexpr int kChienThreads = 1024;   // Chien kernel CTA size
+static constexpr int kChienFastMax = 12;     // locator degrees with an unrolled evaluator
+static constexpr uint16_t kLogZero = 0xFFFF; // stored log of a zero coefficient
 
 struct BchDev {
-  int n, k, t, r, N, words_n, words_k, rw;  // rw = 32-bit words of a parity row
+  int n, k, t, r, m, N, words_n, words_k, rw;  // rw = 32-bit words of the parity
   const uint16_t* exp;   // [2N]
   const uint16_t* log;   // [N + 1]
-  const uint16_t* stab;  // [t][8][256]: odd j = 2s+1, byte position p
-  const uint32_t* erow;  // [k][rw]: x^(r + d) mod g in parity-bit order
+  const uint2* quad;     // [3][8][256]: 4 odd syndromes per entry, byte position p
+  const uint16_t* mul;   // [t][512]: (v * gamma_s), (v << 8) * gamma_s
+  const uint32_t* lf;    // [t][32]: exponent of alpha^(j(n-1-64 lane)) mod N
+  const uint32_t* acol;  // [r][rw]: parity pattern of syndrome bit b
 };
 
-__device__ __forceinline__ uint16_t gf_mul(const BchDev& B, uint16_t a, uint16_t b) {
+// shared-memory image of the syndrome tables
+struct SynTab {
+  const uint2* quad;
+  const uint16_t* mul;
+  const uint32_t* lf;
+};
+
+__device__ __forceinline__ uint32_t gf_mul(const BchDev& B, uint32_t a, uint32_t b) {
   if (!a || !b) return 0;
   return __ldg(&B.exp[__ldg(&B.log[a]) + __ldg(&B.log[b])]);
 }
-// a * alpha^e, 0 <= e < N
-__device__ __forceinline__ uint16_t gf_mul_pow(const BchDev& B, uint16_t a, int e) {
-  if (!a) return 0;
-  return __ldg(&B.exp[__ldg(&B.log[a]) + e]);
+
+__device__ __forceinline__ uint32_t warp_xor(uint32_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
 }
 
-__global__ void __launch_bounds__(kBchWarps * 32) bch_encode_kernel(const BchDev B, const uint64_t* __restrict__ msg,
-                                                                    long long frames, uint64_t* __restrict__ cw) {
-  const int lane = threadIdx.x & 31;
-  const long long warps = (long long)gridDim.x * kBchWarps;
-  for (long long f = (long long)blockIdx.x * kBchWarps + (threadIdx.x >> 5); f < frames; f += warps) {
-    const uint64_t* m = msg + f * B.words_k;
-    uint32_t acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int w = lane; w < B.words_k; w += 32) {
-      uint64_t bits = m[w];
-      if (w == B.words_k - 1 && (B.k & 63)) bits &= (1ull << (B.k & 63)) - 1ull;
-      while (bits) {
-        const int e = __ffsll((long long)bits) - 1;
-        bits &= bits - 1;
-        const uint32_t* row = B.erow + (size_t)(B.k - 1 - (64 * w + e)) * B.rw;
+// Stage the syndrome tables into shared memory; returns the end of the area.
+template <int T>
+__device__ __forceinline__ SynTab load_syn_tables(const BchDev& B, unsigned char* smem) {
+  uint2* q = (uint2*)smem;
+  uint16_t* mu = (uint16_t*)(q + 3 * 8 * 256);
+  uint32_t* lf = (uint32_t*)(mu + T * 512);
+  for (int i = threadIdx.x; i < 3 * 8 * 256; i += blockDim.x) q[i] = B.quad[i];
+  for (int i = threadIdx.x; i < T * 512; i += blockDim.x) mu[i] = B.mul[i];
+  for (int i = threadIdx.x; i < T * 32; i += blockDim.x) lf[i] = B.lf[i];
+  return SynTab{q, mu, lf};
+}
+
+template <int T>
+__host__ __device__ constexpr size_t syn_smem_bytes() {
+  return (size_t)3 * 8 * 256 * 8 + (size_t)T * 512 * 2 + (size_t)T * 32 * 4;
+}
+
+// Odd syndromes S_(2s+1), s < T, of the first `nbits` bits of the packed frame
+// `c` (the remaining codeword bits zero); every lane returns all T values.
+// Words below `copy_words` are also written to `copy` (the last one masked to
+// `copy_bits`).
+template <int T>
+__device__ __forceinline__ void odd_syndromes(const BchDev& B, const SynTab& S, const uint64_t* __restrict__ c,
+                                              int nbits, uint64_t* __restrict__ copy, int copy_bits, int lane,
+                                              uint32_t so[T]) {
+  const int nwords = (nbits + 63) >> 6;
+  const int cwords = (copy_bits + 63) >> 6;
+  uint32_t acc[T];
 #pragma unroll
-        for (int q = 0; q < 6; q++)
-          if (q < B.rw) acc[q] ^= __ldg(&row[q]);
-      }
+  for (int s = 0; s < T; s++) acc[s] = 0;
+  const int U = (nwords + 31) >> 5;
+  for (int u = U - 1; u >= 0; u--) {
+    const int w = lane + 32 * u;
+    uint64_t word = 0;
+    if (w < nwords) {
+      word = __ldg(&c[w]);
+      if (copy && w < cwords) copy[w] = (w == cwords - 1 && (copy_bits & 63)) ? word & ((1ull << (copy_bits & 63)) - 1ull) : word;
+      if (w == nwords - 1 && (nbits & 63)) word &= (1ull << (nbits & 63)) - 1ull;
     }
 #pragma unroll
-    for (int q = 0; q < 6; q++)
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc[q] ^= __shfl_xor_sync(0xffffffffu, acc[q], o);
-    // codeword word w = message bits (< k) | parity bits (k .. n-1)
-    uint64_t* c = cw + f * B.words_n;
-    for (int w = lane; w < B.words_n; w += 32) {
-      const int b0 = 64 * w;
-      uint64_t word = 0;
-      if (b0 < B.k) {
-        word = m[w];
-        if (b0 + 64 > B.k) word &= (1ull << (B.k - b0)) - 1ull;
-      }
-      for (int e = max(0, B.k - b0); e < 64 && b0 + e < B.n; e++) {
-        const int q = b0 + e - B.k;
-        word |= (uint64_t)((acc[q >> 5] >> (q & 31)) & 1u) << e;
-      }
-      c[w] = word;
+    for (int s = 0; s < T; s++) {
+      const uint32_t a = acc[s];
+      acc[s] = (uint32_t)S.mul[s * 512 + (a & 0xffu)] ^ (uint32_t)S.mul[s * 512 + 256 + (a >> 8)];
     }
+    if (word) {
+      const uint32_t lo = (uint32_t)word, hi = (uint32_t)(word >> 32);
+#pragma unroll
+      for (int q = 0; q < (T + 3) / 4; q++) {
+        uint32_t x0 = 0, x1 = 0;
+#pragma unroll
+        for (int p = 0; p < 8; p++) {
+          const uint32_t v = ((p < 4 ? lo : hi) >> (8 * (p & 3))) & 0xffu;
+          const uint2 e = S.quad[(q * 8 + p) * 256 + v];
+          x0 ^= e.x;
+          x1 ^= e.y;
+        }
+        if (4 * q + 0 < T) acc[4 * q + 0] ^= x0 & 0xffffu;
+        if (4 * q + 1 < T) acc[4 * q + 1] ^= x0 >> 16;
+        if (4 * q + 2 < T) acc[4 * q + 2] ^= x1 & 0xffffu;
+        if (4 * q + 3 < T) acc[4 * q + 3] ^= x1 >> 16;
+      }
+    }
+  }
+  // scale by alpha^(j(n-1-64 lane)), then reduce two syndromes per shuffle
+#pragma unroll
+  for (int s = 0; s < T; s++)
+    acc[s] = acc[s] ? __ldg(&B.exp[__ldg(&B.log[acc[s]]) + S.lf[s * 32 + lane]]) : 0u;
+#pragma unroll
+  for (int s = 0; s < T; s += 2) {
+    uint32_t v = acc[s] | (s + 1 < T ? acc[s + 1] << 16 : 0u);
+    v = warp_xor(v);
+    so[s] = v & 0xffffu;
+    if (s + 1 < T) so[s + 1] = v >> 16;
   }
 }
 
-__global__ void __launch_bounds__(kBchWarps * 32) bch_decode_kernel(const BchDev B, const uint64_t* __restrict__ cw,
-                                                                    long long frames, uint64_t* __restrict__ msg,
-                                                                    int32_t* __restrict__ nflips,
-                                                                    uint16_t* __restrict__ synd_out) {
-  extern __shared__ uint16_t s_tab[];  // [t][8][256]
-  for (int i = threadIdx.x; i < B.t * 8 * 256; i += blockDim.x) s_tab[i] = B.stab[i];
+template <int T>
+__global__ void __launch_bounds__(kBchWarps * 32) bch_encode_kernel(const BchDev B, const uint64_t* __restrict__ msg,
+                                                                    long long frames, uint64_t* __restrict__ cw) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const SynTab S = load_syn_tables<T>(B, smem);
+  uint32_t* par_s = (uint32_t*)(smem + syn_smem_bytes<T>());  // [warps][8]
+  uint16_t* syn_s = (uint16_t*)(par_s + kBchWarps * 8);         // [warps][16]
   __syncthreads();
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  uint32_t* par = par_s + wib * 8;
+  uint16_t* sy = syn_s + wib * 16;
   const long long warps = (long long)gridDim.x * kBchWarps;
-  for (long long f = (long long)blockIdx.x * kBchWarps + (threadIdx.x >> 5); f < frames; f += warps) {
-    const uint64_t* c = cw + f * B.words_n;
-    // odd syndromes (partial sums of this lane's words)
-    uint16_t so[kBchMaxT];
+  for (long long f = (long long)blockIdx.x * kBchWarps + wib; f < frames; f += warps) {
+    const uint64_t* m = msg + f * B.words_k;
+    uint64_t* c = cw + f * B.words_n;
+    uint32_t so[T];
+    odd_syndromes<T>(B, S, m, B.k, c, B.k, lane, so);
 #pragma unroll
-    for (int s = 0; s < kBchMaxT; s++) so[s] = 0;
-    for (int w = lane; w < B.words_n; w += 32) {
-      uint64_t word = c[w];
-      if (w == B.words_n - 1 && (B.n & 63)) word &= (1ull << (B.n & 63)) - 1ull;
-      if (!word) continue;
+    for (int s = 0; s < T; s++)
+      if (lane == s) sy[s] = (uint16_t)so[s];
+    __syncwarp();
+    // parity = A s: lane takes syndrome bits b = lane + 32 z
+    uint32_t p[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = lane; b < B.r; b += 32) {
+      if ((sy[b / B.m] >> (b % B.m)) & 1u) {
+        const uint32_t* col = B.acol + (size_t)b * B.rw;
 #pragma unroll
-      for (int s = 0; s < kBchMaxT; s++) {
-        if (s < B.t) {
-          const uint16_t* T = s_tab + s * 2048;
-          uint16_t q = 0;
-#pragma unroll
-          for (int p = 0; p < 8; p++) q ^= T[p * 256 + (int)((word >> (8 * p)) & 0xff)];
-          // * beta^(64 w), beta = alpha^-(2s+1)
-          const long long e = (long long)(B.N - ((64LL * w * (2 * s + 1)) % B.N)) % B.N;
-          so[s] ^= gf_mul_pow(B, q, (int)e);
-        }
+        for (int q = 0; q < 6; q++)
+          if (q < B.rw) p[q] ^= __ldg(&col[q]);
       }
     }
+#pragma unroll
+    for (int q = 0; q < 6; q++) p[q] = warp_xor(p[q]);
+    uint32_t mine = 0;
+#pragma unroll
+    for (int q = 0; q < 6; q++)
+      if (lane == q) mine = p[q];
+    if (lane < 8) par[lane] = mine;
+    __syncwarp();
+    // codeword words from bit k on: parity bit q sits at codeword bit k + q
+    for (int w = (B.k >> 6) + lane; w < B.words_n; w += 32) {
+      const int o = 64 * w - B.k;  // parity bit at the word's bit 0 (negative in the message's tail word)
+      uint64_t word;
+      if (o >= 0) {
+        const int q0 = o >> 5, sh = o & 31;
+        const uint64_t lo = ((uint64_t)par[q0 + 1] << 32) | par[q0];
+        const uint64_t hi = q0 + 2 < 8 ? par[q0 + 2] : 0u;
+        word = sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
+      } else {
+        const uint64_t low = ((uint64_t)par[1] << 32) | par[0];
+        word = (m[w] & ((1ull << (B.k & 63)) - 1ull)) | (low << (-o));
+      }
+      if (w == B.words_n - 1 && (B.n & 63)) word &= (1ull << (B.n & 63)) - 1ull;
+      c[w] = word;
+    }
+    __syncwarp();
+  }
+}
+
+// Kernel 1 of the decoder: syndromes, message copy, Berlekamp-Massey.
+template <int T>
+__global__ void __launch_bounds__(kBchWarps * 32) bch_syndrome_bm_kernel(
+    const BchDev B, const uint64_t* __restrict__ cw, long long frames, uint64_t* __restrict__ msg,
+    int32_t* __restrict__ nflips, uint16_t* __restrict__ synd_out, uint16_t* __restrict__ loc,
+    int32_t* __restrict__ degs) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const SynTab S = load_syn_tables<T>(B, smem);
+  uint16_t* syn_s = (uint16_t*)(smem + syn_smem_bytes<T>());  // [warps][32]
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  uint16_t* sS = syn_s + wib * 32;
+  const long long warps = (long long)gridDim.x * kBchWarps;
+  for (long long f = (long long)blockIdx.x * kBchWarps + wib; f < frames; f += warps) {
+    uint32_t so[T];
+    odd_syndromes<T>(B, S, cw + f * B.words_n, B.n, msg + f * B.words_k, B.k, lane, so);
     uint32_t any = 0;
 #pragma unroll
-    for (int s = 0; s < kBchMaxT; s++) {
-      uint32_t v = so[s];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
-      // * alpha^(j (n-1))
-      so[s] = (s < B.t) ? gf_mul_pow(B, (uint16_t)v, (int)(((long long)(2 * s + 1) * (B.n - 1)) % B.N)) : 0;
+    for (int s = 0; s < T; s++) {
       any |= so[s];
+      if (lane == s) sS[2 * s] = (uint16_t)so[s];
     }
-    // message bits as received
-    uint64_t* mo = msg + f * B.words_k;
-    for (int w = lane; w < B.words_k; w += 32) {
-      uint64_t word = c[w];
-      if (w == B.words_k - 1 && (B.k & 63)) word &= (1ull << (B.k & 63)) - 1ull;
-      mo[w] = word;
+    __syncwarp();
+    // even syndromes: S_(2^a o) = S_o^(2^a)
+    uint32_t ev = 0;
+    const int j = lane + 1;
+    const bool even = lane < 2 * T && !(j & 1);
+    if (even) {
+      const int a = __ffs(j) - 1;
+      const uint32_t so_ = sS[(j >> a) - 1];
+      ev = so_ ? __ldg(&B.exp[((uint32_t)__ldg(&B.log[so_]) << a) % (uint32_t)B.N]) : 0u;
     }
-    __syncwarp();  // the copies are visible to the lanes that flip bits below
-    if (synd_out || any) {
-      uint16_t S[2 * kBchMaxT];  // S[j-1] = S_j
-#pragma unroll
-      for (int j = 1; j <= 2 * kBchMaxT; j++) {
-        if (j & 1) S[j - 1] = so[(j - 1) >> 1];
-        else S[j - 1] = gf_mul(B, S[j / 2 - 1], S[j / 2 - 1]);
+    __syncwarp();
+    if (even) sS[lane] = (uint16_t)ev;
+    __syncwarp();
+    if (synd_out && lane < 2 * T) synd_out[f * 2 * T + lane] = sS[lane];
+    if (!any) {
+      if (lane == 0) {
+        degs[f] = 0;
+        if (nflips) nflips[f] = 0;
       }
-      if (synd_out && lane == 0)
-        for (int j = 0; j < 2 * B.t; j++) synd_out[f * 2 * B.t + j] = S[j];
-      if (!any) {
-        if (lane == 0 && nflips) nflips[f] = 0;
+      __syncwarp();
+      continue;
+    }
+    // Berlekamp-Massey: lane i holds lambda_i and b_i
+    uint32_t lam = lane == 0, bb = lane == 0;
+    int l = 0, mm = 1;
+    for (int nn = 0; nn < 2 * T; nn++) {
+      uint32_t prod = 0;
+      if (lane == 0) prod = sS[nn];
+      else if (lane <= l && lane <= nn) prod = gf_mul(B, lam, sS[nn - lane]);
+      const uint32_t delta = warp_xor(prod);
+      if (delta == 0) {
+        mm += 1;
         continue;
       }
-      // Berlekamp-Massey (BchDecoder::berlekamp_massey), on lane 0
-      uint16_t lam[2 * kBchMaxT + 2];
-      int deg = 0;
-      if (lane == 0) {
-        uint16_t bb[2 * kBchMaxT + 2], tt[2 * kBchMaxT + 2];
-        for (int i = 0; i < 2 * kBchMaxT + 2; i++) lam[i] = bb[i] = 0;
-        lam[0] = bb[0] = 1;
-        int l = 0, m = 1, dl = 0, db = 0;
-        for (int nn = 0; nn < 2 * B.t; nn++) {
-          uint16_t delta = S[nn];
-          for (int i = 1; i <= l; i++)
-            if (i <= dl && nn >= i) delta ^= gf_mul(B, lam[i], S[nn - i]);
-          if (delta == 0) {
-            m += 1;
-            continue;
-          }
-          for (int i = 0; i <= dl; i++) tt[i] = lam[i];
-          const int dt = dl;
-          for (int i = 0; i <= db && m + i < 2 * kBchMaxT + 2; i++) lam[m + i] ^= gf_mul(B, delta, bb[i]);
-          dl = 0;
-          for (int i = 2 * kBchMaxT + 1; i > 0; i--)
-            if (lam[i]) {
-              dl = i;
-              break;
-            }
-          if (2 * l <= nn) {
-            l = nn + 1 - l;
-            const uint16_t di = __ldg(&B.exp[(B.N - __ldg(&B.log[delta])) % B.N]);
-            for (int i = 0; i < 2 * kBchMaxT + 2; i++) bb[i] = 0;
-            db = 0;
-            for (int i = 0; i <= dt; i++) {
-              bb[i] = gf_mul(B, tt[i], di);
-              if (bb[i]) db = i;
-            }
-            m = 1;
-          } else {
-            m += 1;
-          }
-        }
-        deg = dl;
+      const uint32_t tl = lam;
+      const uint32_t bsh = __shfl_up_sync(0xffffffffu, bb, mm);
+      if (lane >= mm) lam ^= gf_mul(B, delta, bsh);
+      if (2 * l <= nn) {
+        l = nn + 1 - l;
+        const uint32_t di = __ldg(&B.exp[(B.N - __ldg(&B.log[delta])) % B.N]);
+        bb = gf_mul(B, tl, di);
+        mm = 1;
+      } else {
+        mm += 1;
       }
-      deg = __shfl_sync(0xffffffffu, deg, 0);
-      // Chien search: lambda(alpha^-i) for degrees i = lane + 32 s
-      int L[2 * kBchMaxT + 2], stepv[2 * kBchMaxT + 2];
-      int roots = 0;
-      if (deg > 0) {
-        for (int j = 0; j <= deg; j++) {
-          const uint32_t lj = __shfl_sync(0xffffffffu, (uint32_t)lam[j], 0);
-          L[j] = lj ? (int)__ldg(&B.log[lj]) : -1;
-          // exponent of the term at i = lane: log(lambda_j) - j * lane (mod N)
-          if (L[j] >= 0) L[j] = (int)(((long long)L[j] - (long long)j * lane % B.N + B.N) % B.N);
-          stepv[j] = (int)((32LL * j) % B.N);
-        }
-        for (int i = lane; i < B.n; i += 32) {
-          uint32_t e = 0;
-          for (int j = 0; j <= deg; j++) {
-            if (L[j] >= 0) {
-              e ^= __ldg(&B.exp[L[j]]);
-              L[j] -= stepv[j];
-              if (L[j] < 0) L[j] += B.N;
-            }
-          }
-          if (e == 0) {
-            roots++;
-            const int bit = B.n - 1 - i;
-            if (bit < B.k) atomicXor((unsigned long long*)&mo[bit >> 6], 1ull << (bit & 63));
-          }
-        }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) roots += __shfl_xor_sync(0xffffffffu, roots, o);
-      if (lane == 0 && nflips) nflips[f] = roots;
-    } else if (lane == 0 && nflips) {
-      nflips[f] = 0;
     }
+    const int deg = 31 - __clz(__ballot_sync(0xffffffffu, lam != 0));
+    loc[f * 32 + lane] = lam ? __ldg(&B.log[lam]) : kLogZero;
+    if (lane == 0) {
+      degs[f] = deg;
+      if (deg == 0 && nflips) nflips[f] = 0;
+    }
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ void flip_root(const BchDev& B, int i, uint64_t* mo) {
+  if (i >= B.r) {
+    const int bit = B.n - 1 - i;
+    atomicXor((unsigned long long*)&mo[bit >> 6], 1ull << (bit & 63));
+  }
+}
+
+// Chien search of a locator of degree D with no zero coefficient below D.
+template <int D>
+__device__ __forceinline__ int chien_fast(const BchDev& B, const uint16_t* __restrict__ sexp, uint32_t myL, int lane,
+                                       uint64_t* mo) {
+  const uint32_t N = (uint32_t)B.N;
+  uint32_t E[D];
+#pragma unroll
+  for (int j = 1; j <= D; j++) {
+    const uint32_t Lj = __shfl_sync(0xffffffffu, myL, j);
+    E[j - 1] = (Lj + N - (uint32_t)(j * lane)) % N;
+  }
+  int roots = 0;
+  const int steps = (B.n + 31) >> 5;
+  for (int s = 0; s < steps; s++) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int j = 1; j <= D; j++) {
+      acc ^= sexp[E[j - 1]];
+      const uint32_t e = E[j - 1] - 32u * j;
+      E[j - 1] = min(e, e + N);
+    }
+    const int i = 32 * s + lane;
+    if (acc == 1u && i < B.n) {
+      roots++;
+      flip_root(B, i, mo);
+    }
+    if ((s & 7) == 7 && (int)__reduce_add_sync(0xffffffffu, (unsigned)roots) == D) break;
+  }
+  return (int)__reduce_add_sync(0xffffffffu, (unsigned)roots);
+}
+
+// Any degree (up to 31) and zero coefficients.
+__device__ __forceinline__ int chien_generic(const BchDev& B, const uint16_t* __restrict__ sexp, uint32_t myL, int deg,
+                                          int lane, uint64_t* mo) {
+  const uint32_t N = (uint32_t)B.N;
+  uint32_t E[31], M[31];
+  for (int j = 1; j <= deg; j++) {
+    const uint32_t Lj = __shfl_sync(0xffffffffu, myL, j);
+    M[j - 1] = Lj == kLogZero ? 0u : 0xffffu;
+    E[j - 1] = Lj == kLogZero ? 0u : (Lj + N - (uint32_t)(j * lane)) % N;
+  }
+  int roots = 0;
+  const int steps = (B.n + 31) >> 5;
+  for (int s = 0; s < steps; s++) {
+    uint32_t acc = 0;
+    for (int j = 1; j <= deg; j++) {
+      acc ^= sexp[E[j - 1]] & M[j - 1];
+      const uint32_t e = E[j - 1] - 32u * j;
+      E[j - 1] = min(e, e + N);
+    }
+    const int i = 32 * s + lane;
+    if (acc == 1u && i < B.n) {
+      roots++;
+      flip_root(B, i, mo);
+    }
+    if ((s & 7) == 7 && (int)__reduce_add_sync(0xffffffffu, (unsigned)roots) == deg) break;
+  }
+  return (int)__reduce_add_sync(0xffffffffu, (unsigned)roots);
+}
+
+// Kernel 2 of the decoder: Chien search of the frames with a nonzero locator.
+__global__ void __launch_bounds__(kChienThreads, 1) bch_chien_kernel(const BchDev B, long long frames,
+                                                                     const uint16_t* __restrict__ loc,
+                                                                     const int32_t* __restrict__ degs,
+                                                                     uint64_t* __restrict__ msg,
+                                                                     int32_t* __restrict__ nflips,
+                                                                     unsigned long long* __restrict__ next) {
+  extern __shared__ __align__(16) uint16_t sexp[];  // alpha^e, e < N
+  for (int i = threadIdx.x; i < B.N; i += blockDim.x) sexp[i] = B.exp[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned long long f = 0;
+    if (lane == 0) f = atomicAdd(next, 1ull);
+    f = __shfl_sync(0xffffffffu, f, 0);
+    if (f >= (unsigned long long)frames) break;
+    const int deg = degs[f];
+    if (deg == 0) continue;
+    const uint32_t myL = loc[f * 32 + lane];
+    const bool zero = lane >= 1 && lane <= deg && myL == kLogZero;
+    uint64_t* mo = msg + f * B.words_k;
+    int roots;
+    if (deg <= kChienFastMax && !__any_sync(0xffffffffu, zero)) {
+      switch (deg) {
+        case 1: roots = chien_fast<1>(B, sexp, myL, lane, mo); break;
+        case 2: roots = chien_fast<2>(B, sexp, myL, lane, mo); break;
+        case 3: roots = chien_fast<3>(B, sexp, myL, lane, mo); break;
+        case 4: roots = chien_fast<4>(B, sexp, myL, lane, mo); break;
+        case 5: roots = chien_fast<5>(B, sexp, myL, lane, mo); break;
+        case 6: roots = chien_fast<6>(B, sexp, myL, lane, mo); break;
+        case 7: roots = chien_fast<7>(B, sexp, myL, lane, mo); break;
+        case 8: roots = chien_fast<8>(B, sexp, myL, lane, mo); break;
+        case 9: roots = chien_fast<9>(B, sexp, myL, lane, mo); break;
+        case 10: roots = chien_fast<10>(B, sexp, myL, lane, mo); break;
+        case 11: roots = chien_fast<11>(B, sexp, myL, lane, mo); break;
+        default: roots = chien_fast<12>(B, sexp, myL, lane, mo); break;
+      }
+    } else {
+      roots = chien_generic(B, sexp, myL, deg, lane, mo);
+    }
+    if (lane == 0 && nflips) nflips[f] = roots;
   }
 }
 
@@ -242,14 +407,17 @@ __global__ void __launch_bounds__(kBchWarps * 32) bch_decode_kernel(const BchDev
 using namespace gf2c;
 
 struct gf2c_bch {
-  int frame = 0, rate = 0, dev = -1;
+  int frame = 0, rate = 0, dev = -1, sms = 148;
+  int occ_syn = 1, occ_enc = 1, occ_chien = 1;
   BchDev d{};
-  std::vector<uint16_t> h_exp, h_log, h_stab;
-  std::vector<uint32_t> h_erow;
+  std::vector<uint16_t> h_exp, h_log, h_mul;
+  std::vector<uint64_t> h_quad;
+  std::vector<uint32_t> h_lf, h_acol;
   std::vector<uint8_t> g;
   std::vector<void*> allocs;
-  void* stage[4] = {nullptr, nullptr, nullptr, nullptr};
-  size_t stage_bytes[4] = {0, 0, 0, 0};
+  static constexpr int kStages = 7;
+  void* stage[kStages] = {};
+  size_t stage_bytes[kStages] = {};
   ~gf2c_bch() {
     for (void* p : allocs) cudaFree(p);
     for (void* p : stage)
@@ -299,25 +467,75 @@ int dev_upload(gf2c_bch* b, const std::vector<T>& v, const T** out) {
   return GF2C_OK;
 }
 
+template <int T>
+size_t enc_smem() { return syn_smem_bytes<T>() + kBchWarps * 8 * 4 + kBchWarps * 16 * 2; }
+template <int T>
+size_t syn_smem() { return syn_smem_bytes<T>() + kBchWarps * 32 * 2; }
+
+template <int T>
+int set_kernel_attrs(gf2c_bch* b) {
+  GF2C_CUDA(cudaFuncSetAttribute(bch_encode_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)enc_smem<T>()));
+  GF2C_CUDA(cudaFuncSetAttribute(bch_syndrome_bm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)syn_smem<T>()));
+  GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ_enc, bch_encode_kernel<T>, kBchWarps * 32,
+                                                          enc_smem<T>()));
+  GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ_syn, bch_syndrome_bm_kernel<T>, kBchWarps * 32,
+                                                          syn_smem<T>()));
+  return GF2C_OK;
+}
+
 int bch_upload(gf2c_bch* b) {
   int dev = 0;
   GF2C_CUDA(cudaGetDevice(&dev));
   if (b->dev == dev) return GF2C_OK;
   if (b->dev >= 0) return set_error(GF2C_ERR_UNSUPPORTED, "BCH code already bound to another device");
   int rc;
+  const uint64_t* quad = nullptr;
   if ((rc = dev_upload(b, b->h_exp, &b->d.exp)) || (rc = dev_upload(b, b->h_log, &b->d.log)) ||
-      (rc = dev_upload(b, b->h_stab, &b->d.stab)) || (rc = dev_upload(b, b->h_erow, &b->d.erow)))
+      (rc = dev_upload(b, b->h_quad, &quad)) || (rc = dev_upload(b, b->h_mul, &b->d.mul)) ||
+      (rc = dev_upload(b, b->h_lf, &b->d.lf)) || (rc = dev_upload(b, b->h_acol, &b->d.acol)))
     return rc;
+  b->d.quad = (const uint2*)quad;
+  GF2C_CUDA(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev));
+  if ((rc = b->d.t == 12 ? set_kernel_attrs<12>(b) : set_kernel_attrs<10>(b))) return rc;
+  const int chien_smem = b->d.N * 2;
+  GF2C_CUDA(cudaFuncSetAttribute(bch_chien_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, chien_smem));
+  GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ_chien, bch_chien_kernel, kChienThreads, chien_smem));
+  b->occ_enc = std::max(b->occ_enc, 1);
+  b->occ_syn = std::max(b->occ_syn, 1);
+  b->occ_chien = std::max(b->occ_chien, 1);
   b->dev = dev;
   return GF2C_OK;
 }
 
-int bch_grid(long long frames) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+int warp_grid(long long frames, int sms, int occ) {
   const long long want = (frames + kBchWarps - 1) / kBchWarps;
-  return (int)std::max<long long>(1, std::min<long long>(want, (long long)sms * 8));
+  return (int)std::max<long long>(1, std::min<long long>(want, (long long)sms * occ));
+}
+
+// Inverse over GF(2) of the r x r matrix given as rows of bits; false if singular.
+bool gf2_invert(int r, std::vector<std::vector<uint64_t>>& rows, std::vector<std::vector<uint64_t>>& inv) {
+  const int W = (r + 63) / 64;
+  inv.assign(r, std::vector<uint64_t>(W, 0));
+  for (int i = 0; i < r; i++) inv[i][i >> 6] |= 1ull << (i & 63);
+  for (int c = 0; c < r; c++) {
+    int piv = -1;
+    for (int i = c; i < r; i++)
+      if ((rows[i][c >> 6] >> (c & 63)) & 1) {
+        piv = i;
+        break;
+      }
+    if (piv < 0) return false;
+    std::swap(rows[c], rows[piv]);
+    std::swap(inv[c], inv[piv]);
+    for (int i = 0; i < r; i++)
+      if (i != c && ((rows[i][c >> 6] >> (c & 63)) & 1))
+        for (int w = 0; w < W; w++) {
+          rows[i][w] ^= rows[c][w];
+          inv[i][w] ^= inv[c][w];
+        }
+  }
+  return true;
 }
 
 }  // namespace
@@ -344,9 +562,9 @@ int gf2c_bch_create_dvbt2(int32_t frame_size, int32_t rate, gf2c_bch** out) {
   d.k = shortf ? kShortK[rate] : kNormalK[rate];
   d.t = shortf ? 12 : kNormalT[rate];
   d.r = d.n - d.k;
-  const int mf = shortf ? 14 : 16;
+  d.m = shortf ? 14 : 16;
   const uint32_t prim = shortf ? 0b100000000101011u : 0b10000000000101101u;
-  const int q = 1 << mf;
+  const int q = 1 << d.m;
   d.N = q - 1;
   d.words_n = (d.n + 63) / 64;
   d.words_k = (d.k + 63) / 64;
@@ -362,12 +580,15 @@ int gf2c_bch_create_dvbt2(int32_t frame_size, int32_t rate, gf2c_bch** out) {
     if (x & (uint32_t)q) x ^= prim;
   }
   for (int e = d.N; e < 2 * d.N; e++) b->h_exp[e] = b->h_exp[e - d.N];
-  auto apow = [&](long long e) { return b->h_exp[((e % d.N) + d.N) % d.N]; };
+  auto apow = [&](long long e) -> uint32_t { return b->h_exp[((e % d.N) + d.N) % d.N]; };
+  auto mul = [&](uint32_t a, uint32_t c) -> uint32_t {
+    return (a && c) ? b->h_exp[b->h_log[a] + b->h_log[c]] : 0u;
+  };
   // generator g = g_1 ... g_t (binary)
   std::vector<uint8_t> g{1};
   for (int i = 0; i < d.t; i++) {
-    std::vector<uint8_t> fct(mf + 1, 0);
-    for (int j = 0; ; j++) {
+    std::vector<uint8_t> fct(d.m + 1, 0);
+    for (int j = 0;; j++) {
       const int e = shortf ? kShortGen[i][j] : kNormalGen[i][j];
       if (e < 0) break;
       fct[e] = 1;
@@ -378,34 +599,50 @@ int gf2c_bch_create_dvbt2(int32_t frame_size, int32_t rate, gf2c_bch** out) {
         for (size_t c = 0; c < fct.size(); c++) p[a + c] ^= fct[c];
     g = p;
   }
-  if ((int)g.size() - 1 != d.r) return set_error(GF2C_ERR_KERNEL, "internal: BCH generator degree mismatch");
+  if ((int)g.size() - 1 != d.r || d.r != d.t * d.m)
+    return set_error(GF2C_ERR_KERNEL, "internal: BCH generator degree mismatch");
   b->g = g;
-  // encoder rows: rem_d = x^(r + d) mod g, parity bit q = coefficient of degree r-1-q
-  b->h_erow.assign((size_t)d.k * d.rw, 0);
-  std::vector<uint8_t> rem(d.r, 0);
-  for (int e = 0; e < d.r; e++) rem[e] = g[e];  // x^r mod g = lower part of g (binary)
-  for (int dd = 0; dd < d.k; dd++) {
-    uint32_t* row = &b->h_erow[(size_t)dd * d.rw];
-    for (int qb = 0; qb < d.r; qb++)
-      if (rem[d.r - 1 - qb]) row[qb >> 5] |= 1u << (qb & 31);
-    const uint8_t top = rem[d.r - 1];  // multiply by x modulo g
-    for (int e = d.r - 1; e > 0; e--) rem[e] = rem[e - 1] ^ (top & g[e]);
-    rem[0] = top & g[0];
-  }
-  // syndrome tables: odd j = 2s+1, beta = alpha^-j, T[s][p][v] = sum_e v_e beta^(8p + e)
-  b->h_stab.assign((size_t)d.t * 8 * 256, 0);
+  // syndrome tables, odd j = 2s+1, beta = alpha^-j
+  b->h_quad.assign((size_t)3 * 8 * 256, 0);
+  b->h_mul.assign((size_t)d.t * 512, 0);
+  b->h_lf.assign((size_t)d.t * 32, 0);
   for (int s = 0; s < d.t; s++) {
-    const int j = 2 * s + 1;
+    const long long j = 2 * s + 1;
     for (int p = 0; p < 8; p++) {
-      uint16_t unit[8];
-      for (int e = 0; e < 8; e++) unit[e] = apow(-(long long)j * (8 * p + e));
+      uint32_t unit[8];
+      for (int e = 0; e < 8; e++) unit[e] = apow(-j * (8 * p + e));
       for (int v = 0; v < 256; v++) {
-        uint16_t acc = 0;
+        uint64_t acc = 0;
         for (int e = 0; e < 8; e++)
           if ((v >> e) & 1) acc ^= unit[e];
-        b->h_stab[((size_t)s * 8 + p) * 256 + v] = acc;
+        b->h_quad[((size_t)(s / 4) * 8 + p) * 256 + v] |= acc << (16 * (s % 4));
       }
     }
+    const uint32_t gamma = apow(-j * 2048);
+    for (int v = 0; v < 256; v++) {
+      b->h_mul[(size_t)s * 512 + v] = (uint16_t)mul((uint32_t)v, gamma);
+      const uint32_t hv = (uint32_t)v << 8;
+      b->h_mul[(size_t)s * 512 + 256 + v] = hv < (uint32_t)q ? (uint16_t)mul(hv, gamma) : 0;
+    }
+    for (int lane = 0; lane < 32; lane++)
+      b->h_lf[(size_t)s * 32 + lane] = (uint32_t)((j * (d.n - 1 - 64 * lane)) % d.N);
+  }
+  // parity from odd syndromes: P[b][q] = bit (b % m) of S_(2(b/m)+1) of parity bit q
+  // (codeword bit k+q, degree r-1-q); A = P^-1, stored by column b
+  {
+    const int W = (d.r + 63) / 64;
+    std::vector<std::vector<uint64_t>> P(d.r, std::vector<uint64_t>(W, 0)), A;
+    for (int qb = 0; qb < d.r; qb++)
+      for (int s = 0; s < d.t; s++) {
+        const uint32_t v = apow((long long)(2 * s + 1) * (d.r - 1 - qb));
+        for (int bp = 0; bp < d.m; bp++)
+          if ((v >> bp) & 1) P[s * d.m + bp][qb >> 6] |= 1ull << (qb & 63);
+      }
+    if (!gf2_invert(d.r, P, A)) return set_error(GF2C_ERR_KERNEL, "internal: BCH parity map is singular");
+    b->h_acol.assign((size_t)d.r * d.rw, 0);
+    for (int qb = 0; qb < d.r; qb++)
+      for (int bb = 0; bb < d.r; bb++)
+        if ((A[qb][bb >> 6] >> (bb & 63)) & 1) b->h_acol[(size_t)bb * d.rw + (qb >> 5)] |= 1u << (qb & 31);
   }
   *out = b.release();
   return GF2C_OK;
@@ -421,7 +658,7 @@ int gf2c_bch_dims(const gf2c_bch* bch, int64_t* n, int64_t* k, int32_t* t, int32
   if (n) *n = bch->d.n;
   if (k) *k = bch->d.k;
   if (t) *t = bch->d.t;
-  if (field_m) *field_m = bch->frame == 1 ? 14 : 16;
+  if (field_m) *field_m = bch->d.m;
   return GF2C_OK;
 }
 
@@ -449,7 +686,9 @@ int gf2c_bch_encode_batch(gf2c_bch* bch, const uint64_t* msg_bits, int64_t frame
     in = (const uint64_t*)bch->stage[0];
     out = (uint64_t*)bch->stage[1];
   }
-  bch_encode_kernel<<<bch_grid(frames), kBchWarps * 32, 0, st>>>(d, in, frames, out);
+  const int grid = warp_grid(frames, bch->sms, bch->occ_enc);
+  if (d.t == 12) bch_encode_kernel<12><<<grid, kBchWarps * 32, enc_smem<12>(), st>>>(d, in, frames, out);
+  else bch_encode_kernel<10><<<grid, kBchWarps * 32, enc_smem<10>(), st>>>(d, in, frames, out);
   GF2C_CUDA(cudaGetLastError());
   if (mem == GF2C_MEM_HOST) {
     GF2C_CUDA(cudaMemcpyAsync(cw_bits, out, bout, cudaMemcpyDeviceToHost, st));
@@ -469,13 +708,16 @@ int gf2c_bch_decode_batch(gf2c_bch* bch, const uint64_t* cw_bits, int64_t frames
   const BchDev& d = bch->d;
   const size_t bin = (size_t)frames * d.words_n * 8, bout = (size_t)frames * d.words_k * 8;
   const size_t bc = (size_t)frames * 4, bs = (size_t)frames * 2 * d.t * 2;
+  if ((rc = bch->ensure_stage(4, (size_t)frames * 32 * 2)) || (rc = bch->ensure_stage(5, (size_t)frames * 4)) ||
+      (rc = bch->ensure_stage(6, 8)))
+    return rc;
   const uint64_t* in = cw_bits;
   uint64_t* out = msg_bits;
   int32_t* cor = corrected;
   uint16_t* syn = syndromes;
   if (mem == GF2C_MEM_HOST) {
-    if ((rc = bch->ensure_stage(0, bin)) || (rc = bch->ensure_stage(1, bout)) || (rc = bch->ensure_stage(2, bc)) ||
-        (rc = bch->ensure_stage(3, bs)))
+    if ((rc = bch->ensure_stage(0, bin)) || (rc = bch->ensure_stage(1, bout)) ||
+        (corrected && (rc = bch->ensure_stage(2, bc))) || (syndromes && (rc = bch->ensure_stage(3, bs))))
       return rc;
     GF2C_CUDA(cudaMemcpyAsync(bch->stage[0], cw_bits, bin, cudaMemcpyHostToDevice, st));
     in = (const uint64_t*)bch->stage[0];
@@ -483,9 +725,18 @@ int gf2c_bch_decode_batch(gf2c_bch* bch, const uint64_t* cw_bits, int64_t frames
     cor = corrected ? (int32_t*)bch->stage[2] : nullptr;
     syn = syndromes ? (uint16_t*)bch->stage[3] : nullptr;
   }
-  const size_t smem = (size_t)d.t * 8 * 256 * sizeof(uint16_t);
-  GF2C_CUDA(cudaFuncSetAttribute(bch_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  bch_decode_kernel<<<bch_grid(frames), kBchWarps * 32, smem, st>>>(d, in, frames, out, cor, syn);
+  uint16_t* loc = (uint16_t*)bch->stage[4];
+  int32_t* degs = (int32_t*)bch->stage[5];
+  unsigned long long* next = (unsigned long long*)bch->stage[6];
+  GF2C_CUDA(cudaMemsetAsync(next, 0, 8, st));
+  const int grid = warp_grid(frames, bch->sms, bch->occ_syn);
+  if (d.t == 12)
+    bch_syndrome_bm_kernel<12><<<grid, kBchWarps * 32, syn_smem<12>(), st>>>(d, in, frames, out, cor, syn, loc, degs);
+  else
+    bch_syndrome_bm_kernel<10><<<grid, kBchWarps * 32, syn_smem<10>(), st>>>(d, in, frames, out, cor, syn, loc, degs);
+  GF2C_CUDA(cudaGetLastError());
+  bch_chien_kernel<<<bch->sms * bch->occ_chien, kChienThreads, (size_t)d.N * 2, st>>>(d, frames, loc, degs, out, cor,
+                                                                                      next);
   GF2C_CUDA(cudaGetLastError());
   if (mem == GF2C_MEM_HOST) {
     GF2C_CUDA(cudaMemcpyAsync(msg_bits, out, bout, cudaMemcpyDeviceToHost, st));
