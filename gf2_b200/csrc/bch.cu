@@ -31,11 +31,14 @@
 //    locator and of the correction polynomial (the discrepancy is a warp XOR
 //    reduction).  It stores the locator as logarithms per frame.
 //  * Decoder, kernel 2 (Chien search): the antilog table of the field in
-//    shared memory; lane l evaluates positions i = l + 32s with the terms'
+//    shared memory, stored with an offset so that the exponents are reduced
+//    mod N once per 8 position steps and the steps in between are constant
+//    load offsets; lane l evaluates positions i = l + 32s with the terms'
 //    exponents in registers (locator degrees 1..12 unrolled); a root i flips
 //    bit n-1-i when it lies in the message.  A frame stops once it has found
 //    deg(lambda) roots (a polynomial has no more), which returns the same
-//    roots as the full search.  Frames are taken from an atomic counter.
+//    roots as the full search.  Kernel 1 files each frame under its locator
+//    degree; kernel 2 takes the frames degree by degree, highest first.
 #include <algorithm>
 #include <cstring>
 #include <memory>
@@ -48,6 +51,8 @@ namespace gf2c {
 static constexpr int kBchWarps = 8;          // warps per CTA in the syndrome kernels
 static constexpr int kChienThreads = 1024;   // Chien kernel CTA size
 static constexpr int kChienFastMax = 12;     // locator degrees with an unrolled evaluator
+static constexpr int kChienSeg = 8;          // positions steps between exponent reductions
+static constexpr int kChienOff = 32 * kChienFastMax * kChienSeg;  // antilog table offset
 static constexpr uint16_t kLogZero = 0xFFFF; // stored log of a zero coefficient
 
 struct BchDev {
@@ -218,7 +223,7 @@ template <int T>
 __global__ void __launch_bounds__(kBchWarps * 32) bch_syndrome_bm_kernel(
     const BchDev B, const uint64_t* __restrict__ cw, long long frames, uint64_t* __restrict__ msg,
     int32_t* __restrict__ nflips, uint16_t* __restrict__ synd_out, uint16_t* __restrict__ loc,
-    int32_t* __restrict__ degs) {
+    int32_t* __restrict__ degs, uint32_t* __restrict__ bcnt, int32_t* __restrict__ blist) {
   extern __shared__ __align__(16) unsigned char smem[];
   const SynTab S = load_syn_tables<T>(B, smem);
   uint16_t* syn_s = (uint16_t*)(smem + syn_smem_bytes<T>());  // [warps][32]
@@ -282,10 +287,17 @@ __global__ void __launch_bounds__(kBchWarps * 32) bch_syndrome_bm_kernel(
       }
     }
     const int deg = 31 - __clz(__ballot_sync(0xffffffffu, lam != 0));
+    const bool zero_coef = __any_sync(0xffffffffu, lane >= 1 && lane <= deg && lam == 0);
     loc[f * 32 + lane] = lam ? __ldg(&B.log[lam]) : kLogZero;
     if (lane == 0) {
       degs[f] = deg;
-      if (deg == 0 && nflips) nflips[f] = 0;
+      if (deg == 0) {
+        if (nflips) nflips[f] = 0;
+      } else {  // Chien work list of the frame's bucket: its degree, or 0 for the generic evaluator
+        const int bk = (deg <= kChienFastMax && !zero_coef) ? deg : 0;
+        const uint32_t pos = atomicAdd(&bcnt[bk], 1u);
+        blist[(size_t)bk * frames + pos] = (int32_t)f;
+      }
     }
     __syncwarp();
   }
@@ -299,32 +311,40 @@ __device__ __forceinline__ void flip_root(const BchDev& B, int i, uint64_t* mo) 
 }
 
 // Chien search of a locator of degree D with no zero coefficient below D.
+// sexp[x] = alpha^(x - kChienOff); term j keeps Ep = (its exponent mod N) +
+// kChienOff, which stays in [0, N + kChienOff) over a segment of kChienSeg
+// steps of -32 j each, so the steps inside a segment are constant offsets of
+// the load and the reduction mod N happens once per segment.
 template <int D>
 __device__ __forceinline__ int chien_fast(const BchDev& B, const uint16_t* __restrict__ sexp, uint32_t myL, int lane,
-                                       uint64_t* mo) {
+                                          uint64_t* mo) {
   const uint32_t N = (uint32_t)B.N;
-  uint32_t E[D];
+  uint32_t Ep[D];
 #pragma unroll
   for (int j = 1; j <= D; j++) {
     const uint32_t Lj = __shfl_sync(0xffffffffu, myL, j);
-    E[j - 1] = (Lj + N - (uint32_t)(j * lane)) % N;
+    Ep[j - 1] = (Lj + N - (uint32_t)(j * lane)) % N + kChienOff;
   }
   int roots = 0;
   const int steps = (B.n + 31) >> 5;
-  for (int s = 0; s < steps; s++) {
-    uint32_t acc = 0;
+  for (int s0 = 0; s0 < steps; s0 += kChienSeg) {
+#pragma unroll
+    for (int g = 0; g < kChienSeg; g++) {
+      uint32_t acc = 0;
+#pragma unroll
+      for (int j = 1; j <= D; j++) acc ^= sexp[Ep[j - 1] - 32u * j * g];
+      const int i = 32 * (s0 + g) + lane;
+      if (acc == 1u && i < B.n) {
+        roots++;
+        flip_root(B, i, mo);
+      }
+    }
 #pragma unroll
     for (int j = 1; j <= D; j++) {
-      acc ^= sexp[E[j - 1]];
-      const uint32_t e = E[j - 1] - 32u * j;
-      E[j - 1] = min(e, e + N);
+      const uint32_t e = Ep[j - 1] - 32u * j * kChienSeg;
+      Ep[j - 1] = e < (uint32_t)kChienOff ? e + N : e;
     }
-    const int i = 32 * s + lane;
-    if (acc == 1u && i < B.n) {
-      roots++;
-      flip_root(B, i, mo);
-    }
-    if ((s & 7) == 7 && (int)__reduce_add_sync(0xffffffffu, (unsigned)roots) == D) break;
+    if ((int)__reduce_add_sync(0xffffffffu, (unsigned)roots) == D) break;
   }
   return (int)__reduce_add_sync(0xffffffffu, (unsigned)roots);
 }
@@ -344,7 +364,7 @@ __device__ __forceinline__ int chien_generic(const BchDev& B, const uint16_t* __
   for (int s = 0; s < steps; s++) {
     uint32_t acc = 0;
     for (int j = 1; j <= deg; j++) {
-      acc ^= sexp[E[j - 1]] & M[j - 1];
+      acc ^= sexp[E[j - 1] + kChienOff] & M[j - 1];
       const uint32_t e = E[j - 1] - 32u * j;
       E[j - 1] = min(e, e + N);
     }
@@ -359,44 +379,53 @@ __device__ __forceinline__ int chien_generic(const BchDev& B, const uint16_t* __
 }
 
 // Kernel 2 of the decoder: Chien search of the frames with a nonzero locator.
+// Work is taken from the per-degree lists in the order generic, 12, 11, ..., 1,
+// so the warps of an SM mostly run the same unrolled evaluator (one
+// instruction stream) and the longest frames start first.
 __global__ void __launch_bounds__(kChienThreads, 1) bch_chien_kernel(const BchDev B, long long frames,
                                                                      const uint16_t* __restrict__ loc,
                                                                      const int32_t* __restrict__ degs,
+                                                                     const uint32_t* __restrict__ bcnt,
+                                                                     const int32_t* __restrict__ blist,
                                                                      uint64_t* __restrict__ msg,
                                                                      int32_t* __restrict__ nflips,
                                                                      unsigned long long* __restrict__ next) {
-  extern __shared__ __align__(16) uint16_t sexp[];  // alpha^e, e < N
-  for (int i = threadIdx.x; i < B.N; i += blockDim.x) sexp[i] = B.exp[i];
+  extern __shared__ __align__(16) uint16_t sexp[];  // [N + kChienOff]: alpha^(x - kChienOff)
+  __shared__ long long s_pre[kChienFastMax + 2];     // work offsets of the buckets in fetch order
+  for (int i = threadIdx.x; i < B.N + kChienOff; i += blockDim.x) sexp[i] = B.exp[i + B.N - kChienOff];
+  if (threadIdx.x == 0) {
+    s_pre[0] = 0;
+    for (int k = 0; k <= kChienFastMax; k++) s_pre[k + 1] = s_pre[k] + bcnt[k == 0 ? 0 : kChienFastMax + 1 - k];
+  }
   __syncthreads();
+  const long long total = s_pre[kChienFastMax + 1];
   const int lane = threadIdx.x & 31;
   for (;;) {
-    unsigned long long f = 0;
-    if (lane == 0) f = atomicAdd(next, 1ull);
-    f = __shfl_sync(0xffffffffu, f, 0);
-    if (f >= (unsigned long long)frames) break;
-    const int deg = degs[f];
-    if (deg == 0) continue;
+    unsigned long long w = 0;
+    if (lane == 0) w = atomicAdd(next, 1ull);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if ((long long)w >= total) break;
+    int k = 0;
+    while ((long long)w >= s_pre[k + 1]) k++;
+    const int bk = k == 0 ? 0 : kChienFastMax + 1 - k;
+    const long long f = blist[(size_t)bk * frames + (size_t)((long long)w - s_pre[k])];
     const uint32_t myL = loc[f * 32 + lane];
-    const bool zero = lane >= 1 && lane <= deg && myL == kLogZero;
     uint64_t* mo = msg + f * B.words_k;
     int roots;
-    if (deg <= kChienFastMax && !__any_sync(0xffffffffu, zero)) {
-      switch (deg) {
-        case 1: roots = chien_fast<1>(B, sexp, myL, lane, mo); break;
-        case 2: roots = chien_fast<2>(B, sexp, myL, lane, mo); break;
-        case 3: roots = chien_fast<3>(B, sexp, myL, lane, mo); break;
-        case 4: roots = chien_fast<4>(B, sexp, myL, lane, mo); break;
-        case 5: roots = chien_fast<5>(B, sexp, myL, lane, mo); break;
-        case 6: roots = chien_fast<6>(B, sexp, myL, lane, mo); break;
-        case 7: roots = chien_fast<7>(B, sexp, myL, lane, mo); break;
-        case 8: roots = chien_fast<8>(B, sexp, myL, lane, mo); break;
-        case 9: roots = chien_fast<9>(B, sexp, myL, lane, mo); break;
-        case 10: roots = chien_fast<10>(B, sexp, myL, lane, mo); break;
-        case 11: roots = chien_fast<11>(B, sexp, myL, lane, mo); break;
-        default: roots = chien_fast<12>(B, sexp, myL, lane, mo); break;
-      }
-    } else {
-      roots = chien_generic(B, sexp, myL, deg, lane, mo);
+    switch (bk) {
+      case 1: roots = chien_fast<1>(B, sexp, myL, lane, mo); break;
+      case 2: roots = chien_fast<2>(B, sexp, myL, lane, mo); break;
+      case 3: roots = chien_fast<3>(B, sexp, myL, lane, mo); break;
+      case 4: roots = chien_fast<4>(B, sexp, myL, lane, mo); break;
+      case 5: roots = chien_fast<5>(B, sexp, myL, lane, mo); break;
+      case 6: roots = chien_fast<6>(B, sexp, myL, lane, mo); break;
+      case 7: roots = chien_fast<7>(B, sexp, myL, lane, mo); break;
+      case 8: roots = chien_fast<8>(B, sexp, myL, lane, mo); break;
+      case 9: roots = chien_fast<9>(B, sexp, myL, lane, mo); break;
+      case 10: roots = chien_fast<10>(B, sexp, myL, lane, mo); break;
+      case 11: roots = chien_fast<11>(B, sexp, myL, lane, mo); break;
+      case 12: roots = chien_fast<12>(B, sexp, myL, lane, mo); break;
+      default: roots = chien_generic(B, sexp, myL, degs[f], lane, mo); break;
     }
     if (lane == 0 && nflips) nflips[f] = roots;
   }
@@ -415,7 +444,7 @@ struct gf2c_bch {
   std::vector<uint32_t> h_lf, h_acol;
   std::vector<uint8_t> g;
   std::vector<void*> allocs;
-  static constexpr int kStages = 7;
+  static constexpr int kStages = 8;
   void* stage[kStages] = {};
   size_t stage_bytes[kStages] = {};
   ~gf2c_bch() {
@@ -498,7 +527,7 @@ int bch_upload(gf2c_bch* b) {
   b->d.quad = (const uint2*)quad;
   GF2C_CUDA(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev));
   if ((rc = b->d.t == 12 ? set_kernel_attrs<12>(b) : set_kernel_attrs<10>(b))) return rc;
-  const int chien_smem = b->d.N * 2;
+  const int chien_smem = (b->d.N + kChienOff) * 2;
   GF2C_CUDA(cudaFuncSetAttribute(bch_chien_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, chien_smem));
   GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ_chien, bch_chien_kernel, kChienThreads, chien_smem));
   b->occ_enc = std::max(b->occ_enc, 1);
@@ -709,7 +738,7 @@ int gf2c_bch_decode_batch(gf2c_bch* bch, const uint64_t* cw_bits, int64_t frames
   const size_t bin = (size_t)frames * d.words_n * 8, bout = (size_t)frames * d.words_k * 8;
   const size_t bc = (size_t)frames * 4, bs = (size_t)frames * 2 * d.t * 2;
   if ((rc = bch->ensure_stage(4, (size_t)frames * 32 * 2)) || (rc = bch->ensure_stage(5, (size_t)frames * 4)) ||
-      (rc = bch->ensure_stage(6, 8)))
+      (rc = bch->ensure_stage(6, 128)) || (rc = bch->ensure_stage(7, (size_t)(kChienFastMax + 1) * frames * 4)))
     return rc;
   const uint64_t* in = cw_bits;
   uint64_t* out = msg_bits;
@@ -727,16 +756,18 @@ int gf2c_bch_decode_batch(gf2c_bch* bch, const uint64_t* cw_bits, int64_t frames
   }
   uint16_t* loc = (uint16_t*)bch->stage[4];
   int32_t* degs = (int32_t*)bch->stage[5];
-  unsigned long long* next = (unsigned long long*)bch->stage[6];
-  GF2C_CUDA(cudaMemsetAsync(next, 0, 8, st));
+  unsigned long long* next = (unsigned long long*)bch->stage[6];  // work counter, then bucket sizes
+  uint32_t* bcnt = (uint32_t*)((char*)bch->stage[6] + 64);
+  int32_t* blist = (int32_t*)bch->stage[7];
+  GF2C_CUDA(cudaMemsetAsync(bch->stage[6], 0, 128, st));
   const int grid = warp_grid(frames, bch->sms, bch->occ_syn);
   if (d.t == 12)
-    bch_syndrome_bm_kernel<12><<<grid, kBchWarps * 32, syn_smem<12>(), st>>>(d, in, frames, out, cor, syn, loc, degs);
+    bch_syndrome_bm_kernel<12><<<grid, kBchWarps * 32, syn_smem<12>(), st>>>(d, in, frames, out, cor, syn, loc, degs, bcnt, blist);
   else
-    bch_syndrome_bm_kernel<10><<<grid, kBchWarps * 32, syn_smem<10>(), st>>>(d, in, frames, out, cor, syn, loc, degs);
+    bch_syndrome_bm_kernel<10><<<grid, kBchWarps * 32, syn_smem<10>(), st>>>(d, in, frames, out, cor, syn, loc, degs, bcnt, blist);
   GF2C_CUDA(cudaGetLastError());
-  bch_chien_kernel<<<bch->sms * bch->occ_chien, kChienThreads, (size_t)d.N * 2, st>>>(d, frames, loc, degs, out, cor,
-                                                                                      next);
+  bch_chien_kernel<<<bch->sms * bch->occ_chien, kChienThreads, (size_t)(d.N + kChienOff) * 2, st>>>(
+      d, frames, loc, degs, bcnt, blist, out, cor, next);
   GF2C_CUDA(cudaGetLastError());
   if (mem == GF2C_MEM_HOST) {
     GF2C_CUDA(cudaMemcpyAsync(msg_bits, out, bout, cudaMemcpyDeviceToHost, st));
