@@ -39,6 +39,10 @@ EXPORTS = [
     "gf2c_adam_step", "gf2c_count_errors",
     "gf2c_bch_create_dvbt2", "gf2c_bch_destroy", "gf2c_bch_dims", "gf2c_bch_generator",
     "gf2c_bch_encode_batch", "gf2c_bch_decode_batch",
+    "gf2c_io_probe", "gf2c_io_write_bitvec", "gf2c_io_read_bitvec", "gf2c_io_write_bitmatrix",
+    "gf2c_io_read_bitmatrix", "gf2c_io_write_sparse", "gf2c_io_read_sparse", "gf2c_code_create_file",
+    "gf2c_io_write_code", "gf2c_siphash13", "gf2c_code_cache_hash", "gf2c_code_parity_part",
+    "gf2c_dense_encoder_create", "gf2c_dense_encoder_destroy", "gf2c_dense_encode_batch",
 ]
 
 
@@ -107,6 +111,22 @@ def _load():
     L.gf2c_bch_generator.argtypes = [_vp, _vp]
     L.gf2c_bch_encode_batch.argtypes = [_vp, _vp, _i64, _vp, _i32, _vp]
     L.gf2c_bch_decode_batch.argtypes = [_vp, _vp, _i64, _vp, _vp, _vp, _i32, _vp]
+    _s = ctypes.c_char_p
+    L.gf2c_io_probe.argtypes = [_s, _vp, _vp, _vp]
+    L.gf2c_io_write_bitvec.argtypes = [_s, _vp, _i64, _i32]
+    L.gf2c_io_read_bitvec.argtypes = [_s, _vp, _i64, _vp]
+    L.gf2c_io_write_bitmatrix.argtypes = [_s, _vp, _i64, _i64, _i32]
+    L.gf2c_io_read_bitmatrix.argtypes = [_s, _i32, _vp, _i64, _vp, _vp]
+    L.gf2c_io_write_sparse.argtypes = [_s, _i32, _i64, _i64, _vp, _vp, _i32]
+    L.gf2c_io_read_sparse.argtypes = [_s, _i32, _vp, _vp, _vp, _vp, _vp, _i64]
+    L.gf2c_code_create_file.argtypes = [_s, ctypes.POINTER(_vp)]
+    L.gf2c_io_write_code.argtypes = [_s, _vp, _i32, _i32]
+    L.gf2c_siphash13.argtypes = [_vp, _i64, _u64, _u64, _vp]
+    L.gf2c_code_cache_hash.argtypes = [_vp, _vp]
+    L.gf2c_code_parity_part.argtypes = [_vp, _vp]
+    L.gf2c_dense_encoder_create.argtypes = [_vp, _i64, _i64, ctypes.POINTER(_vp)]
+    L.gf2c_dense_encoder_destroy.argtypes = [_vp]
+    L.gf2c_dense_encode_batch.argtypes = [_vp, _vp, _i64, _vp, _i32, _vp]
     return L
 
 

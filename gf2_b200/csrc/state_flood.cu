@@ -198,24 +198,20 @@ __device__ __forceinline__ void sf_var_pass(const uint4* st, const Post<ALL_SMEM
     const int u = CH.x * vgs + j;
     if (j >= vgs || u >= n) continue;
     float b = lu[u];
-    {
-      const int* __restrict__ ci = sci + V.y + j;
-      int i = 0;
-      for (; i + 4 <= V.x; i += 4) {
-        int e[4];
-        uint4 s[4];
+    const int* __restrict__ ci = sci + V.y + j;
+    // batches of 4 edges, the last one partial: the edge-table loads of a
+    // batch, then its state gathers, are in flight together (two dependent
+    // round trips per batch, whatever the degree)
+    for (int i = 0; i < V.x; i += 4) {
+      int e[4];
+      uint4 s[4];
 #pragma unroll
-        for (int q = 0; q < 4; q++) e[q] = __ldg(&ci[(i + q) * vgs]);
+      for (int q = 0; q < 4; q++) e[q] = i + q < V.x ? __ldg(&ci[(i + q) * vgs]) : -1;
 #pragma unroll
-        for (int q = 0; q < 4; q++) s[q] = st[e[q] < 0 ? 0 : (e[q] & 0xffffff)];
+      for (int q = 0; q < 4; q++) s[q] = st[e[q] < 0 ? 0 : (e[q] & 0xffffff)];
 #pragma unroll
-        for (int q = 0; q < 4; q++)
-          if (e[q] >= 0) b = __fadd_rn(b, state_c2v(s[q], e[q] >> 24));
-      }
-      for (; i < V.x; i++) {
-        const int e0 = __ldg(&ci[i * vgs]);
-        if (e0 >= 0) b = __fadd_rn(b, state_c2v(st[e0 & 0xffffff], e0 >> 24));
-      }
+      for (int q = 0; q < 4; q++)
+        if (e[q] >= 0) b = __fadd_rn(b, state_c2v(s[q], e[q] >> 24));
     }
     *P.at(u) = b;
   }

@@ -262,6 +262,57 @@ int gf2c_bch_encode_batch(gf2c_bch* bch, const uint64_t* msg_bits, int64_t frame
 int gf2c_bch_decode_batch(gf2c_bch* bch, const uint64_t* cw_bits, int64_t frames, uint64_t* msg_bits,
                           int32_t* corrected, uint16_t* syndromes, int32_t mem, void* stream);
 
+/* ------------------------------------------------------------------------
+ * gf2 file formats and the LDPC encoder cache (host side).
+ * Binary "GF2DATA" files (crates/gf2-core/src/io/format.rs:1-16,
+ * header.rs:6-82): 32-byte header, compact JSON metadata, little-endian payload;
+ * type tags 1 BitVec (io/bitvec.rs), 2 BitMatrix (io/matrix.rs),
+ * 3 SpBitMatrix (COO pairs, io/sparse.rs), 4 SpBitMatrixDual (CSR + CSC).
+ * format: 0 binary, 1 text, 2 hex (io/formats.rs); -1 on input = detect as
+ * SerializationFormat::detect does.  Bits are packed BitVec words; a
+ * BitMatrix is rows x ceil(cols/64) words, row-major.
+ * ------------------------------------------------------------------------ */
+/* SerializationFormat::detect + the header / metadata: type tag (1..4), format,
+ * dims3 = {len_bits} (BitVec), {rows, cols} (BitMatrix), {rows, cols, nnz}. */
+int gf2c_io_probe(const char* path, int32_t* type_tag, int32_t* format, int64_t* dims3);
+/* BitVec::save_to_file_with_format / load_from_file (auto-detect) (io/bitvec.rs). */
+int gf2c_io_write_bitvec(const char* path, const uint64_t* words, int64_t len_bits, int32_t format);
+int gf2c_io_read_bitvec(const char* path, uint64_t* words, int64_t cap_words, int64_t* len_bits);
+/* BitMatrix::save_to_file_with_format / load_from_file_with_format (io/matrix.rs). */
+int gf2c_io_write_bitmatrix(const char* path, const uint64_t* words, int64_t rows, int64_t cols, int32_t format);
+int gf2c_io_read_bitmatrix(const char* path, int32_t format, uint64_t* words, int64_t cap_words, int64_t* rows,
+                           int64_t* cols);
+/* SpBitMatrix (type 3) / SpBitMatrixDual (type 4) save (binary or text) and
+ * load (io/sparse.rs): CSR with ascending columns; loading a COO file sorts
+ * and removes repeated edges (SpBitMatrix::from_coo_deduplicated).  Pass
+ * row_ptr / col_idx NULL to query rows / cols / nnz first. */
+int gf2c_io_write_sparse(const char* path, int32_t type_tag, int64_t rows, int64_t cols, const int64_t* row_ptr,
+                         const int64_t* col_idx, int32_t format);
+int gf2c_io_read_sparse(const char* path, int32_t format, int64_t* rows, int64_t* cols, int64_t* nnz,
+                        int64_t* row_ptr, int64_t* col_idx, int64_t cap_nnz);
+/* LdpcCode from / to a parity-check matrix file (type 3 or 4). */
+int gf2c_code_create_file(const char* path, gf2c_code** out);
+int gf2c_io_write_code(const char* path, const gf2c_code* code, int32_t type_tag, int32_t format);
+/* SipHash-1-3 (the algorithm of Rust's DefaultHasher; zero keys there). */
+int gf2c_siphash13(const void* data, int64_t len, uint64_t k0, uint64_t k1, uint64_t* out);
+/* CacheKey::from_params (ldpc/encoding/cache.rs:84-90, 461-487): the
+ * structural hash of H that names the cache file "n{n}_k{k}_h{hash:x}.gf2". */
+int gf2c_code_cache_hash(const gf2c_code* code, uint64_t* hash);
+/* RuEncodingMatrices::parity_part (richardson_urbanke.rs:372): P, k x
+ * ceil((n-k)/64) words, row i = the parity bits of message bit i, for the
+ * systematic form with the message in columns [0, k) (what the cache files
+ * hold); GF2C_ERR_UNSUPPORTED for a code whose systematic columns differ. */
+int gf2c_code_parity_part(const gf2c_code* code, uint64_t* words);
+/* Encoding with a dense parity part (RuEncodingMatrices::encode /
+ * encode_batch, richardson_urbanke.rs:263-330, as reconstructed by
+ * EncodingCache::from_directory, cache.rs:347-433): codeword = [message |
+ * P^T message].  P is copied at creation (host words). */
+typedef struct gf2c_dense_encoder gf2c_dense_encoder;
+int gf2c_dense_encoder_create(const uint64_t* parity_words, int64_t k, int64_t n, gf2c_dense_encoder** out);
+int gf2c_dense_encoder_destroy(gf2c_dense_encoder* enc);
+int gf2c_dense_encode_batch(gf2c_dense_encoder* enc, const uint64_t* msg_bits, int64_t frames, uint64_t* cw_bits,
+                            int32_t mem, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
