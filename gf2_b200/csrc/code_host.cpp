@@ -367,6 +367,27 @@ int build_dvbt2(int frame, int rate, HostCode& c) {
   c.kind = 2;
   c.z = (int)Z;
   c.q = (int)q;
+  // encoder lists: address x of block b lies in row group x mod q and rotates
+  // the block's 360 bits by x div q; repeated addresses cancel (XOR)
+  {
+    std::vector<std::vector<int>> rg(q);
+    for (int b = 0; b < T.rows; b++) {
+      std::vector<int64_t> xs(T.addr + T.row_ptr[b], T.addr + T.row_ptr[b + 1]);
+      std::sort(xs.begin(), xs.end());
+      for (size_t i = 0; i < xs.size();) {
+        size_t j = i;
+        while (j < xs.size() && xs[j] == xs[i]) j++;
+        if ((j - i) & 1) rg[xs[i] % q].push_back((b << 16) | (int)(xs[i] / q));
+        i = j;
+      }
+    }
+    c.enc_rg_ptr.assign(1, 0);
+    c.enc_rg_ent.clear();
+    for (const auto& v : rg) {
+      c.enc_rg_ent.insert(c.enc_rg_ent.end(), v.begin(), v.end());
+      c.enc_rg_ptr.push_back((int)c.enc_rg_ent.size());
+    }
+  }
   c.dvb_index = frame * 6 + rate;
   // Row group a = checks p = a + q t (t = 0..359).  An address x lies in row
   // group x mod q and, for info block b, links check t to bit b*360 + (t - x div q) mod 360:
@@ -570,6 +591,11 @@ int upload_code(HostCode& c) {
     if ((rc = dev_copy(c, rp, &d.csr_ptr))) return rc;
     if ((rc = dev_copy(c, ri, &d.csr_idx))) return rc;
     d.enc_kind = c.kind == 2 ? 0 : 1;
+    if (c.kind == 2) {
+      d.enc_q = c.q;
+      if ((rc = dev_copy(c, c.enc_rg_ptr, &d.enc_rg_ptr))) return rc;
+      if ((rc = dev_copy(c, c.enc_rg_ent, &d.enc_rg_ent))) return rc;
+    }
     c.dev = d;
     c.dev_id = dev;
   }

@@ -4,9 +4,11 @@
 // (RuEncodingMatrices::encode, crates/gf2-coding/src/ldpc/encoding/richardson_urbanke.rs:263-289,
 // 97.5% of its encode time in BitMatrix::matvec_transpose).  For DVB-T2 codes the
 // parity part of H is the staircase, so the same unique codeword is
-//   s = H_info u (one XOR per info edge),  p[i] = s[0] ^ ... ^ s[i]
-// i.e. an XOR-gather followed by a prefix-XOR scan, done here with warp ballots
-// and a block scan over 32-bit words.  Other codes use the dense generator
+//   s = H_info u,  p[i] = s[0] ^ ... ^ s[i].
+// With the checks of row group a = p mod q at positions t = p div q, s of a
+// row group is a XOR of the 360-bit info blocks rotated by their addresses
+// (32-bit windows), and p is a prefix over row groups plus a prefix along t;
+// a warp-shuffle bit transpose puts the parity into natural order.  Other codes use the dense generator
 // block of the right-to-left pivot search (the reference's columns).
 //
 // Syndrome: LdpcCode::syndrome (crates/gf2-coding/src/ldpc/core.rs:129-133).
@@ -17,7 +19,8 @@
 
 namespace gf2c {
 
-static constexpr int kEncThreads = 1024;
+static constexpr int kEncThreads = 1024;     // channel kernel (Philox + LLRs for one frame)
+static constexpr int kEncodeThreads = 256;   // encode kernel (several frames per SM)
 
 // Bit i of a u32-word bit array.
 __device__ __forceinline__ uint32_t getbit(const uint32_t* w, int i) { return (w[i >> 5] >> (i & 31)) & 1u; }
@@ -43,67 +46,126 @@ __device__ __forceinline__ uint32_t block_xor_scan_excl(uint32_t bit, uint32_t* 
   return r;
 }
 
+// 32 x 32 bit transpose across a warp: lane c returns bit r = bit c of lane r's x.
+template <int J, uint32_t M>
+__device__ __forceinline__ uint32_t transpose_step(uint32_t x, int lane) {
+  const uint32_t y = __shfl_xor_sync(0xffffffffu, x, J);
+  return (lane & J) ? ((x & ~M) | ((y >> J) & M)) : ((x & M) | ((y & M) << J));
+}
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, int lane) {
+  x = transpose_step<16, 0x0000ffffu>(x, lane);
+  x = transpose_step<8, 0x00ff00ffu>(x, lane);
+  x = transpose_step<4, 0x0f0f0f0fu>(x, lane);
+  x = transpose_step<2, 0x33333333u>(x, lane);
+  return transpose_step<1, 0x55555555u>(x, lane);
+}
+
 // Encodes the message bits u (k bits, u32 words in shared memory) into the
-// codeword cw (n bits, u32 words in shared memory).  scratch: >= words32(m) + 64 words.
+// codeword cw (n bits, u32 words in shared memory); scratch as encode_smem sizes it.
 __device__ void encode_frame(const DevCode& C, const uint32_t* u, uint32_t* cw, uint32_t* scratch) {
   const int n = C.n, k = C.k, m = C.m;
-  const int wn = (n + 31) >> 5, wk = (k + 31) >> 5, wm = (m + 31) >> 5;
-  uint32_t* par = scratch;          // m parity bits
-  uint32_t* warp_tot = scratch + wm;
+  const int wn = (n + 31) >> 5, wk = (k + 31) >> 5;
   if (C.enc_kind == 0) {
-    // s_p = XOR of the info bits of check p (natural check order)
-    for (int base = 0; base < m; base += blockDim.x) {
-      const int p = base + threadIdx.x;
-      uint32_t s = 0;
-      if (p < m) {
-        const int e1 = __ldg(&C.csr_ptr[p + 1]);
-        for (int e = __ldg(&C.csr_ptr[p]); e < e1; e++) {
-          const int v = __ldg(&C.csr_idx[e]);
-          if (v < k) s ^= getbit(u, v);
+    // Row group a holds checks p = a + q t (t < 360).  Its info syndrome,
+    // S_a[t] = XOR over its addresses x = a + q tau (block b) of u[360 b + (t - tau) mod 360],
+    // is a XOR of the info blocks rotated by tau: one 32-bit window per word
+    // and address, from a cyclic copy of each block.
+    const int q = C.enc_q, nblk = k / 360;
+    uint32_t* U2 = scratch;        // per info block, 23 words: bit j = block bit j mod 360 (j < 736)
+    uint32_t* S = U2 + 23 * nblk;  // q x 12 words (t = 32 w + bit)
+    uint32_t* ctot = S + 12 * q;   // XOR over all row groups
+    uint32_t* cpre = ctot + 12;    // exclusive prefix of ctot along t
+    // codeword: the message, zero parity (the parity bits are OR-ed in below)
+    for (int w = threadIdx.x; w < wn; w += blockDim.x) {
+      const int lo = 32 * w;
+      cw[w] = lo + 32 <= k ? u[w] : (lo < k ? u[w] & ((1u << (k - lo)) - 1u) : 0u);
+    }
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+      const int base = (360 * b) >> 5, sh = (360 * b) & 31;
+      uint32_t x[12];
+#pragma unroll
+      for (int i = 0; i < 12; i++) {
+        const uint32_t lo = u[base + i], hi = base + i + 1 < wk ? u[base + i + 1] : 0u;
+        x[i] = __funnelshift_r(lo, hi, sh);
+      }
+      x[11] = (x[11] & 0xffu) | (x[0] << 8);  // block bits 352..359, then 0..23
+      uint32_t* d = U2 + 23 * b;
+#pragma unroll
+      for (int i = 0; i < 12; i++) d[i] = x[i];
+#pragma unroll
+      for (int i = 12; i < 23; i++) d[i] = __funnelshift_r(x[i - 12], x[i - 11], 24);
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < 12 * q; idx += blockDim.x) {
+      const int a = idx / 12, w = idx - 12 * a;
+      uint32_t acc = 0;
+      const int e1 = __ldg(&C.enc_rg_ptr[a + 1]);
+      for (int e = __ldg(&C.enc_rg_ptr[a]); e < e1; e++) {
+        const int ent = __ldg(&C.enc_rg_ent[e]);
+        int s = 32 * w - (ent & 0xffff);
+        if (s < 0) s += 360;
+        const uint32_t* d = U2 + 23 * (ent >> 16) + (s >> 5);
+        acc ^= __funnelshift_r(d[0], d[1], s & 31);
+      }
+      S[idx] = w == 11 ? acc & 0xffu : acc;
+    }
+    __syncthreads();
+    // parity bit p = a + q t is the XOR of the info syndromes of all checks up
+    // to p in natural order: (all row groups at t' < t) ^ (row groups a' <= a at t)
+    {
+      const int lane = threadIdx.x & 31;
+      for (int w = threadIdx.x >> 5; w < 12; w += blockDim.x >> 5) {  // one warp per word: XOR scan over a
+        uint32_t carry = 0;
+        for (int a0 = 0; a0 < q; a0 += 32) {
+          const int a = a0 + lane;
+          uint32_t v = a < q ? S[12 * a + w] : 0u;
+#pragma unroll
+          for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, v, d);
+            if (lane >= d) v ^= y;
+          }
+          v ^= carry;
+          if (a < q) S[12 * a + w] = v;
+          carry = __shfl_sync(0xffffffffu, v, 31);
+        }
+        if (lane == 0) ctot[w] = carry;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t carry = 0;
+      for (int w = 0; w < 12; w++) {
+        const uint32_t x = ctot[w];
+        uint32_t inc = x;
+        inc ^= inc << 1;
+        inc ^= inc << 2;
+        inc ^= inc << 4;
+        inc ^= inc << 8;
+        inc ^= inc << 16;
+        inc ^= carry;
+        cpre[w] = inc ^ x;
+        carry = (inc >> 31) ? ~0u : 0u;
+      }
+    }
+    __syncthreads();
+    // natural order: 32 row groups x 32 positions per warp task, transposed in
+    // registers; column t goes to codeword bit k + t q + 32 A
+    const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5, nA = (q + 31) >> 5;
+    for (int task = threadIdx.x >> 5; task < 12 * nA; task += nwarps) {
+      const int A = task / 12, T = task - 12 * A;
+      const int a = 32 * A + lane;
+      uint32_t x = a < q ? S[12 * a + T] ^ cpre[T] : 0u;
+      x = transpose32(x, lane);
+      const int t = 32 * T + lane;
+      if (t < 360) {
+        const int nb = min(32, q - 32 * A);
+        const uint32_t seg = nb < 32 ? x & ((1u << nb) - 1u) : x;
+        const int p0 = k + t * q + 32 * A, w0 = p0 >> 5, sh = p0 & 31;
+        if (seg) {
+          atomicOr(&cw[w0], seg << sh);
+          if (sh && (seg >> (32 - sh))) atomicOr(&cw[w0 + 1], seg >> (32 - sh));
         }
       }
-      const uint32_t b = __ballot_sync(0xffffffffu, s);
-      if ((threadIdx.x & 31) == 0 && p < m) par[p >> 5] = b;
-    }
-    __syncthreads();
-    // prefix XOR over the m bits: in-word scan, then carry across words
-    for (int base = 0; base < wm; base += blockDim.x) {
-      const int w = base + threadIdx.x;
-      uint32_t x = w < wm ? par[w] : 0u;
-      x ^= x << 1;
-      x ^= x << 2;
-      x ^= x << 4;
-      x ^= x << 8;
-      x ^= x << 16;
-      const uint32_t carry_in = base > 0 ? (par[base - 1] >> 31) & 1u : 0u;
-      __syncthreads();
-      const uint32_t ex = block_xor_scan_excl(x >> 31, warp_tot) ^ carry_in;
-      if (w < wm) par[w] = ex ? ~x : x;
-      __syncthreads();
-    }
-    if (m & 31) {
-      if (threadIdx.x == 0) par[wm - 1] &= (1u << (m & 31)) - 1u;
-    }
-    __syncthreads();
-    // cw = [u | par]
-    for (int w = threadIdx.x; w < wn; w += blockDim.x) {
-      uint32_t out = 0;
-      const int lo = 32 * w;
-      if (lo + 32 <= k) {
-        out = u[w];
-      } else {
-        if (lo < k) out = u[w] & ((1u << (k - lo)) - 1u);
-        // parity bits p at codeword positions k + p
-        const int pstart = lo < k ? 0 : lo - k;     // first parity index in this word
-        const int bitpos = lo < k ? k - lo : 0;     // its bit position in this word
-        const int pw = pstart >> 5, ps = pstart & 31;
-        uint64_t two = (uint64_t)par[pw] | ((pw + 1 < wm) ? ((uint64_t)par[pw + 1] << 32) : 0ull);
-        uint32_t bits = (uint32_t)(two >> ps);
-        if (bitpos < 32) out |= bits << bitpos;
-        const int valid = n - lo;
-        if (valid < 32) out &= (1u << valid) - 1u;
-      }
-      cw[w] = out;
     }
     __syncthreads();
   } else {
@@ -136,11 +198,11 @@ __device__ void encode_frame(const DevCode& C, const uint32_t* u, uint32_t* cw, 
 // shared memory: u (wk32) + cw (wn32) + scratch (max(wm32 + 64, 2*Wm))
 static size_t encode_smem(const DevCode& C) {
   const int wn = (C.n + 31) / 32, wk = (C.k + 31) / 32, wm = (C.m + 31) / 32;
-  const int scratch = std::max(wm + 64, 2 * C.words_m);
+  const int scratch = std::max(std::max(wm + 64, 2 * C.words_m), C.enc_kind == 0 ? 23 * (C.k / 360) + 12 * C.enc_q + 24 : 0);
   return (size_t)(((wk + 3) & ~3) + ((wn + 3) & ~3) + scratch + 4) * 4;
 }
 
-__global__ void __launch_bounds__(kEncThreads) encode_kernel(const DevCode* __restrict__ Cp,
+__global__ void __launch_bounds__(kEncodeThreads) encode_kernel(const DevCode* __restrict__ Cp,
                                                              const uint64_t* __restrict__ msg,
                                                              long long frames, uint64_t* __restrict__ cw) {
   extern __shared__ __align__(16) uint32_t sm[];
@@ -323,7 +385,12 @@ int launch_encode(const DevCode* dcode, const DevCode& h, const uint64_t* msg, l
   if (frames <= 0) return GF2C_OK;
   size_t smem = encode_smem(h);
   GF2C_CUDA(cudaFuncSetAttribute(encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  encode_kernel<<<grid_for(frames), kEncThreads, smem, st>>>(dcode, msg, frames, cw);
+  int dev = 0, sms = 148, per_sm = 1;
+  GF2C_CUDA(cudaGetDevice(&dev));
+  GF2C_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, encode_kernel, kEncodeThreads, smem));
+  const long long grid = std::max<long long>(1, std::min<long long>(frames, (long long)sms * std::max(per_sm, 1)));
+  encode_kernel<<<(int)grid, kEncodeThreads, smem, st>>>(dcode, msg, frames, cw);
   GF2C_CUDA(cudaGetLastError());
   return GF2C_OK;
 }

@@ -75,6 +75,9 @@ struct DevCode {
   const uint64_t* enc_p;           // kind 1: k rows of words_m words (parity j of row i)
   const int* enc_msg_cols;         // kind 1: k message columns
   const int* enc_par_cols;         // kind 1: m parity columns
+  int enc_q;                       // kind 0: row groups (m / 360)
+  const int* enc_rg_ptr;           // kind 0: q + 1 offsets into enc_rg_ent
+  const int* enc_rg_ent;           // kind 0: info block b << 16 | rotation tau, per row group
 };
 
 uint64_t next_code_serial();
@@ -118,6 +121,7 @@ struct HostCode {
   int enc_status = GF2C_OK;
   std::vector<uint64_t> enc_p;
   std::vector<int> enc_msg_cols, enc_par_cols;
+  std::vector<int> enc_rg_ptr, enc_rg_ent;  // DVB-T2: per row group a, (block, rotation) of its info addresses
 
   // device copy (lazily uploaded per device)
   std::mutex dev_mu;
