@@ -1,8 +1,13 @@
 // Example / self-check of the C++ API (gf2cuda.hpp).
-//   example codes   -- host-only: builds codes, checks dimensions and errors
-//   example decode  -- GPU: restated decoder tests of crates/gf2-coding/src/ldpc/core.rs
+//   example codes   -- host-only: builds codes, checks dimensions and errors, BCH
+//                      parameters, gf2 file roundtrips and the encoder cache
+//   example decode  -- GPU: restated decoder tests of crates/gf2-coding/src/ldpc/core.rs,
+//                      BCH correction, cached-parity encoding
+#include <unistd.h>
+
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 
 #include "gf2cuda.hpp"
 
@@ -30,6 +35,48 @@ static int codes() {
     threw = true;
   }
   EXPECT(threw);
+  // BCH parameters (bch/dvb_t2/params.rs tests): generator degree t m
+  auto bch = gf2::BchCode::dvb_t2(0, gf2::CodeRate::Rate2_3);
+  EXPECT(bch.n() == 43200 && bch.k() == 43040 && bch.t() == 10 && bch.field_m() == 16);
+  EXPECT(bch.generator().size() == 161 && bch.generator()[160] == 1);
+  EXPECT(gf2::BchCode::dvb_t2(1, gf2::CodeRate::Rate1_2).generator().size() == 169);
+  // gf2 files: roundtrips and the cache file name
+  const std::string dir = std::filesystem::temp_directory_path() / ("gf2cpp_" + std::to_string(::getpid()));
+  std::filesystem::create_directories(dir);
+  gf2::BitVec v = gf2::BitVec::zeros(100);
+  v.set(3, true);
+  v.set(99, true);
+  for (int fmt = 0; fmt < 3; fmt++) {
+    gf2::io::save_bitvec(dir + "/v", v, fmt);
+    EXPECT(gf2::io::load_bitvec(dir + "/v") == v);
+  }
+  s.save(dir + "/h.gf2");
+  auto s2 = gf2::LdpcCode::from_file(dir + "/h.gf2");
+  EXPECT(s2.n() == s.n() && s2.k() == s.k());
+  gf2::EncodingCache cache;
+  const auto& P = cache.get_or_compute(s);
+  EXPECT(P.rows == 7200 && P.cols == 9000);
+  gf2::BitVec cw = gf2::BitVec::zeros(s.n());
+  cw.set(17, true);
+  for (size_t j = 0; j < P.cols; j++) cw.set(7200 + j, P.get(17, j));
+  {  // H cw = 0 on the host, from the CSR
+    std::vector<int64_t> ptr(s.m() + 1);
+    int64_t nnz = 0;
+    gf2::check(gf2c_code_dims(s.handle(), nullptr, nullptr, nullptr, &nnz, nullptr));
+    std::vector<int64_t> idx((size_t)nnz);
+    gf2::check(gf2c_code_csr(s.handle(), ptr.data(), idx.data()));
+    for (size_t r = 0; r < s.m(); r++) {
+      bool par = false;
+      for (int64_t e = ptr[r]; e < ptr[r + 1]; e++) par ^= cw.get((size_t)idx[e]);
+      EXPECT(!par);
+    }
+  }
+  cache.save_to_directory(dir + "/cache");
+  auto loaded = gf2::EncodingCache::from_directory(dir + "/cache");
+  EXPECT(loaded.size() == 1);
+  const auto name = gf2::EncodingCache::filename(gf2::EncodingCache::key(s));
+  EXPECT(name.rfind("n16200_k7200_h", 0) == 0 && std::filesystem::exists(dir + "/cache/" + name));
+  std::filesystem::remove_all(dir);
   std::printf("codes ok\n");
   return 0;
 }
@@ -62,6 +109,19 @@ static int decode() {
   for (size_t i = 0; i < s.n(); i++) l[i] = Llr(c.get(i) ? -4.0f : 4.0f);
   r = ds.decode_iterative(l, 20);
   EXPECT(r.converged && r.decoded_bits == msg);
+  // outer BCH: t errors corrected (bch/dvb_t2/mod.rs roundtrip tests)
+  auto bch = gf2::BchCode::dvb_t2(1, gf2::CodeRate::Rate1_2);
+  gf2::BitVec bm = gf2::BitVec::zeros(bch.k());
+  for (size_t i = 0; i < bch.k(); i += 5) bm.set(i, true);
+  auto bc = gf2::BchEncoder(bch).encode(bm);
+  EXPECT(bc.len() == bch.n());
+  for (size_t e = 0; e < bch.t(); e++) bc.set(97 * e + 11, !bc.get(97 * e + 11));
+  std::vector<int32_t> corrected;
+  auto bd = gf2::BchDecoder(bch).decode_batch({bc}, &corrected);
+  EXPECT(bd[0] == bm && corrected[0] == (int32_t)bch.t());
+  // encoding from the cached parity part equals the encoder's codeword
+  gf2::EncodingCache cache;
+  EXPECT(cache.encoder(s).encode(msg) == c);
   std::printf("decode ok\n");
   return 0;
 }
