@@ -73,6 +73,7 @@ SINGLE = {
 }
 WORKLOADS = sorted(list(SINGLE) + ["c3", "c5", "bch"])
 BCH_METRIC = "BCH decoded info Gbit/s on 1 B200 (DVB-T2 outer code, hard decision)"
+BCH_DATA = "synthetic (seeded random messages, BCH-encoded, f mod 13 random bit errors per frame)"
 BCH_DESC = ("dvbt2-normal-3/5 outer BCH (n=38880, k=38688, t=12) hard-decision decode, 65536 frames, "
             "frame f carries f mod 13 random bit errors (0..t, every frame corrected)")
 
@@ -636,7 +637,8 @@ def main():
             decoder, metric = "reference flooding min-sum (CPU restatement)", METRIC
         line = {"metric": metric, "value": gbps, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox AWGN frames)",
+                "vs_baseline": None, "dtype": "u16" if args.workload == "bch" else "f32",
+                "data": BCH_DATA if args.workload == "bch" else "synthetic (seeded Philox AWGN frames)",
                 "config": {"workload": desc, "decoder": decoder},
                 "cpu_baseline": {"value": gbps, "unit": UNIT, "cores": info["cores"], "kind": "port",
                                  "sample": info["sample"]},
@@ -729,7 +731,8 @@ def main():
                 "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype,
-                "data": "synthetic (seeded Philox AWGN frames, BPSK, encoder output)", "config": config,
+                "data": BCH_DATA if args.workload == "bch" else "synthetic (seeded Philox AWGN frames, BPSK, encoder output)",
+                "config": config,
                 "iterations": iters,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": read_traffic(args.workload),
