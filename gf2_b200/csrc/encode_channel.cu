@@ -60,19 +60,83 @@ __device__ __forceinline__ uint32_t transpose32(uint32_t x, int lane) {
   return transpose_step<1, 0x55555555u>(x, lane);
 }
 
+// DVB-T2 structure (row group a holds the checks p = a + q t, t < 360): the
+// info syndrome of row group a is
+//   S_a[t] = XOR over its addresses x = a + q tau (info block b) of u[360 b + (t - tau) mod 360],
+// a XOR of the info blocks rotated by tau, i.e. one 32-bit window per word and
+// address taken from a cyclic copy of each block.
+
+// Cyclic copies of the info blocks: 23 words per block, bit j = block bit j mod 360.
+__device__ __forceinline__ void dvbt2_build_blocks(const uint32_t* u, int wk, int nblk, uint32_t* U2) {
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    const int base = (360 * b) >> 5, sh = (360 * b) & 31;
+    uint32_t x[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) {
+      const uint32_t lo = u[base + i], hi = base + i + 1 < wk ? u[base + i + 1] : 0u;
+      x[i] = __funnelshift_r(lo, hi, sh);
+    }
+    x[11] = (x[11] & 0xffu) | (x[0] << 8);  // block bits 352..359, then 0..23
+    uint32_t* d = U2 + 23 * b;
+#pragma unroll
+    for (int i = 0; i < 12; i++) d[i] = x[i];
+#pragma unroll
+    for (int i = 12; i < 23; i++) d[i] = __funnelshift_r(x[i - 12], x[i - 11], 24);
+  }
+}
+
+// S[12 a + w] = word w (t = 32 w + bit) of the info syndrome of row group a.
+__device__ __forceinline__ void dvbt2_row_syndromes(const DevCode& C, const uint32_t* U2, int q, uint32_t* S) {
+  for (int idx = threadIdx.x; idx < 12 * q; idx += blockDim.x) {
+    const int a = idx / 12, w = idx - 12 * a;
+    uint32_t acc = 0;
+    const int e1 = __ldg(&C.enc_rg_ptr[a + 1]);
+    for (int e = __ldg(&C.enc_rg_ptr[a]); e < e1; e++) {
+      const int ent = __ldg(&C.enc_rg_ent[e]);
+      int s = 32 * w - (ent & 0xffff);
+      if (s < 0) s += 360;
+      const uint32_t* d = U2 + 23 * (ent >> 16) + (s >> 5);
+      acc ^= __funnelshift_r(d[0], d[1], s & 31);
+    }
+    S[idx] = w == 11 ? acc & 0xffu : acc;
+  }
+}
+
+// OR bit t of row vector a (X[12 a + w] ^ xor_t[w]; xor_t nullable) into
+// dst at bit offset + t q + a (natural order): 32 row groups x 32 positions
+// per warp task, transposed in registers.  dst starts at zero there.
+__device__ __forceinline__ void dvbt2_scatter_natural(const uint32_t* X, const uint32_t* xor_t, int q, uint32_t* dst,
+                                                      int offset) {
+  const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5, nA = (q + 31) >> 5;
+  for (int task = threadIdx.x >> 5; task < 12 * nA; task += nwarps) {
+    const int A = task / 12, T = task - 12 * A;
+    const int a = 32 * A + lane;
+    uint32_t x = a < q ? X[12 * a + T] ^ (xor_t ? xor_t[T] : 0u) : 0u;
+    x = transpose32(x, lane);
+    const int t = 32 * T + lane;
+    if (t < 360) {
+      const int nb = min(32, q - 32 * A);
+      const uint32_t seg = nb < 32 ? x & ((1u << nb) - 1u) : x;
+      const int p0 = offset + t * q + 32 * A, w0 = p0 >> 5, sh = p0 & 31;
+      if (seg) {
+        atomicOr(&dst[w0], seg << sh);
+        if (sh && (seg >> (32 - sh))) atomicOr(&dst[w0 + 1], seg >> (32 - sh));
+      }
+    }
+  }
+}
+
 // Encodes the message bits u (k bits, u32 words in shared memory) into the
 // codeword cw (n bits, u32 words in shared memory); scratch as encode_smem sizes it.
 __device__ void encode_frame(const DevCode& C, const uint32_t* u, uint32_t* cw, uint32_t* scratch) {
   const int n = C.n, k = C.k, m = C.m;
   const int wn = (n + 31) >> 5, wk = (k + 31) >> 5;
   if (C.enc_kind == 0) {
-    // Row group a holds checks p = a + q t (t < 360).  Its info syndrome,
-    // S_a[t] = XOR over its addresses x = a + q tau (block b) of u[360 b + (t - tau) mod 360],
-    // is a XOR of the info blocks rotated by tau: one 32-bit window per word
-    // and address, from a cyclic copy of each block.
+    // parity bit p = a + q t is the XOR of the info syndromes of all checks up
+    // to p in natural order: (all row groups at t' < t) ^ (row groups a' <= a at t)
     const int q = C.enc_q, nblk = k / 360;
-    uint32_t* U2 = scratch;        // per info block, 23 words: bit j = block bit j mod 360 (j < 736)
-    uint32_t* S = U2 + 23 * nblk;  // q x 12 words (t = 32 w + bit)
+    uint32_t* U2 = scratch;        // cyclic info blocks
+    uint32_t* S = U2 + 23 * nblk;  // row-group syndromes, then their prefix over a
     uint32_t* ctot = S + 12 * q;   // XOR over all row groups
     uint32_t* cpre = ctot + 12;    // exclusive prefix of ctot along t
     // codeword: the message, zero parity (the parity bits are OR-ed in below)
@@ -80,38 +144,10 @@ __device__ void encode_frame(const DevCode& C, const uint32_t* u, uint32_t* cw, 
       const int lo = 32 * w;
       cw[w] = lo + 32 <= k ? u[w] : (lo < k ? u[w] & ((1u << (k - lo)) - 1u) : 0u);
     }
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-      const int base = (360 * b) >> 5, sh = (360 * b) & 31;
-      uint32_t x[12];
-#pragma unroll
-      for (int i = 0; i < 12; i++) {
-        const uint32_t lo = u[base + i], hi = base + i + 1 < wk ? u[base + i + 1] : 0u;
-        x[i] = __funnelshift_r(lo, hi, sh);
-      }
-      x[11] = (x[11] & 0xffu) | (x[0] << 8);  // block bits 352..359, then 0..23
-      uint32_t* d = U2 + 23 * b;
-#pragma unroll
-      for (int i = 0; i < 12; i++) d[i] = x[i];
-#pragma unroll
-      for (int i = 12; i < 23; i++) d[i] = __funnelshift_r(x[i - 12], x[i - 11], 24);
-    }
+    dvbt2_build_blocks(u, wk, nblk, U2);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < 12 * q; idx += blockDim.x) {
-      const int a = idx / 12, w = idx - 12 * a;
-      uint32_t acc = 0;
-      const int e1 = __ldg(&C.enc_rg_ptr[a + 1]);
-      for (int e = __ldg(&C.enc_rg_ptr[a]); e < e1; e++) {
-        const int ent = __ldg(&C.enc_rg_ent[e]);
-        int s = 32 * w - (ent & 0xffff);
-        if (s < 0) s += 360;
-        const uint32_t* d = U2 + 23 * (ent >> 16) + (s >> 5);
-        acc ^= __funnelshift_r(d[0], d[1], s & 31);
-      }
-      S[idx] = w == 11 ? acc & 0xffu : acc;
-    }
+    dvbt2_row_syndromes(C, U2, q, S);
     __syncthreads();
-    // parity bit p = a + q t is the XOR of the info syndromes of all checks up
-    // to p in natural order: (all row groups at t' < t) ^ (row groups a' <= a at t)
     {
       const int lane = threadIdx.x & 31;
       for (int w = threadIdx.x >> 5; w < 12; w += blockDim.x >> 5) {  // one warp per word: XOR scan over a
@@ -148,25 +184,7 @@ __device__ void encode_frame(const DevCode& C, const uint32_t* u, uint32_t* cw, 
       }
     }
     __syncthreads();
-    // natural order: 32 row groups x 32 positions per warp task, transposed in
-    // registers; column t goes to codeword bit k + t q + 32 A
-    const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5, nA = (q + 31) >> 5;
-    for (int task = threadIdx.x >> 5; task < 12 * nA; task += nwarps) {
-      const int A = task / 12, T = task - 12 * A;
-      const int a = 32 * A + lane;
-      uint32_t x = a < q ? S[12 * a + T] ^ cpre[T] : 0u;
-      x = transpose32(x, lane);
-      const int t = 32 * T + lane;
-      if (t < 360) {
-        const int nb = min(32, q - 32 * A);
-        const uint32_t seg = nb < 32 ? x & ((1u << nb) - 1u) : x;
-        const int p0 = k + t * q + 32 * A, w0 = p0 >> 5, sh = p0 & 31;
-        if (seg) {
-          atomicOr(&cw[w0], seg << sh);
-          if (sh && (seg >> (32 - sh))) atomicOr(&cw[w0 + 1], seg >> (32 - sh));
-        }
-      }
-    }
+    dvbt2_scatter_natural(S, cpre, q, cw, k);
     __syncthreads();
   } else {
     // parity word j (64 bits) = XOR over message bits i of P[i][j]
@@ -241,6 +259,39 @@ __global__ void __launch_bounds__(256) syndrome_kernel(const DevCode* __restrict
     __syncthreads();
     uint32_t* so = synd ? (uint32_t*)(synd + f * (long long)C.words_m) : nullptr;
     int cnt = 0;
+    if (C.enc_kind == 0) {
+      // s_p = (info syndrome of check p) ^ c[k + p] ^ c[k + p - 1], natural order
+      const int k = C.k, m = C.m, q = C.enc_q, nblk = k / 360, wm = (m + 31) >> 5;
+      uint32_t* U2 = sm + wn;
+      uint32_t* S = U2 + 23 * nblk;
+      uint32_t* nat = S + 12 * q;  // wm words
+      for (int w = threadIdx.x; w < wm; w += blockDim.x) nat[w] = 0u;
+      dvbt2_build_blocks(sm, (k + 31) >> 5, nblk, U2);
+      __syncthreads();
+      dvbt2_row_syndromes(C, U2, q, S);
+      __syncthreads();
+      dvbt2_scatter_natural(S, nullptr, q, nat, 0);
+      __syncthreads();
+      auto par_word = [&](int w) -> uint32_t {  // codeword bits k + 32 w .. + 31
+        const int pos = k + 32 * w, i = pos >> 5;
+        return __funnelshift_r(sm[i], i + 1 < wn ? sm[i + 1] : 0u, pos & 31);
+      };
+      for (int w = threadIdx.x; w < 2 * C.words_m; w += blockDim.x) {
+        uint32_t x = 0;
+        if (w < wm) {
+          const uint32_t pw = par_word(w), prev = w > 0 ? par_word(w - 1) : 0u;
+          x = nat[w] ^ pw ^ ((pw << 1) | (prev >> 31));
+          if (w == wm - 1 && (m & 31)) x &= (1u << (m & 31)) - 1u;
+        }
+        cnt += __popc(x);
+        if (so) so[w] = x;
+      }
+      atomicAdd(&s_w, cnt);
+      __syncthreads();
+      if (threadIdx.x == 0 && weight) weight[f] = s_w;
+      __syncthreads();
+      continue;
+    }
     for (int base = 0; base < 32 * 2 * C.words_m; base += blockDim.x) {
       const int p = base + threadIdx.x;
       uint32_t s = 0;
@@ -399,6 +450,7 @@ int launch_syndrome(const DevCode* dcode, const DevCode& h, const uint64_t* cw, 
                     uint64_t* synd, int32_t* weight, cudaStream_t st) {
   if (frames <= 0) return GF2C_OK;
   size_t smem = (size_t)((h.n + 31) / 32) * 4;
+  if (h.enc_kind == 0) smem += (size_t)(23 * (h.k / 360) + 12 * h.enc_q + (h.m + 31) / 32) * 4;
   GF2C_CUDA(cudaFuncSetAttribute(syndrome_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   syndrome_kernel<<<grid_for(frames), 256, smem, st>>>(dcode, cw, frames, synd, weight);
   GF2C_CUDA(cudaGetLastError());
