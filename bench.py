@@ -31,6 +31,8 @@ Workloads (one "step" = one decode of the whole batch):
                 65536 packed words, frame f with f mod 13 random bit errors;
                 syndromes, Berlekamp-Massey and Chien search on the device
                 (metric: BCH decoded info Gbit/s).
+  enc           DVB-T2 normal 3/5 LDPC encoder, 65536 packed random messages
+                (metric: LDPC encoded info Gbit/s).
 
 The LLR input of every workload is larger than L2 (no flush needed).
 `--impl reference` times the reference decoder's CPU restatement (flooding
@@ -71,11 +73,25 @@ SINGLE = {
                   desc="dvbt2-short-1/2 flooding min-sum fp32 (reference decoder), 256 frames, "
                        "Eb/N0 1.0 dB, max 50 it"),
 }
-WORKLOADS = sorted(list(SINGLE) + ["c3", "c5", "bch"])
+WORKLOADS = sorted(list(SINGLE) + ["c3", "c5", "bch", "enc"])
 BCH_METRIC = "BCH decoded info Gbit/s on 1 B200 (DVB-T2 outer code, hard decision)"
 BCH_DATA = "synthetic (seeded random messages, BCH-encoded, f mod 13 random bit errors per frame)"
 BCH_DESC = ("dvbt2-normal-3/5 outer BCH (n=38880, k=38688, t=12) hard-decision decode, 65536 frames, "
             "frame f carries f mod 13 random bit errors (0..t, every frame corrected)")
+ENC_METRIC = "LDPC encoded info Gbit/s on 1 B200 (DVB-T2 encoder)"
+ENC_DATA = "synthetic (seeded random messages)"
+ENC_DESC = "dvbt2-normal-3/5 LDPC encode (k=38880 -> n=64800), 65536 frames of random messages"
+
+
+def metric_of(w):
+    return {"bch": BCH_METRIC, "enc": ENC_METRIC}.get(w, METRIC)
+
+
+def data_of(w, gpu_arm):
+    if w in ("bch", "enc"):
+        return BCH_DATA if w == "bch" else ENC_DATA
+    return ("synthetic (seeded Philox AWGN frames, BPSK, encoder output)" if gpu_arm
+            else "synthetic (seeded Philox AWGN frames)")
 
 
 def parse():
@@ -609,6 +625,93 @@ def run_cpu_bch(steps, warmup, cores=None, frames=None):
     return gbps, dict(cores=cores, sample=sample, frames=S)
 
 
+class EncBatch:
+    """DVB-T2 normal 3/5 LDPC encode of a device batch of packed messages."""
+
+    def __init__(self, dev, rank, frames):
+        import torch
+
+        import gf2_b200 as g
+        from gf2_b200 import _capi as C
+        self.g, self.C, self.torch = g, C, torch
+        self.frames = frames or 65536
+        self.code = g.LdpcCode.dvb_t2_normal(1)
+        k, n, F = self.code.k(), self.code.n(), self.frames
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(3000 + rank)
+        m = torch.randint(-2 ** 31, 2 ** 31, (F, 2 * g.words(k)), dtype=torch.int32, device=dev, generator=gen)
+        self.msg = m.view(torch.int64)
+        if k & 63:
+            self.msg[:, -1] &= (1 << (k & 63)) - 1
+        self.out = torch.zeros((F, g.words(n)), dtype=torch.int64, device=dev)
+        self.stream = torch.cuda.current_stream(dev)
+        self.desc = ENC_DESC
+        self.dtype = "u32"
+
+    def step(self):
+        from gf2_b200.ldpc import _ptr, _stream_ptr
+        self.C.check(self.C.lib.gf2c_encode_batch(self.code.handle, _ptr(self.msg), self.frames, _ptr(self.out),
+                                                  self.C.MEM_DEVICE, _stream_ptr(self.stream)))
+
+    def launches(self):
+        return 1
+
+    def bits_per_step(self):
+        return self.frames * self.code.k()
+
+    def stats(self):
+        g, c = self.g, self.code
+        s, w = c.syndrome_batch(self.out[:256].contiguous())
+        self.torch.cuda.synchronize()
+        per = 8 * g.words(c.k()) + 8 * g.words(c.n())
+        return self.frames * per, {"codewords_checked": 256, "all_valid": bool((w.cpu() == 0).all())
+                                   if hasattr(w, "cpu") else bool((w == 0).all())}
+
+    def host_step_factory(self):
+        """The public C-ABI host path: pinned packed messages in, codewords out."""
+        import ctypes
+
+        torch, g, C, c, F = self.torch, self.g, self.C, self.code, self.frames
+        h_msg = torch.empty_like(self.msg, device="cpu").pin_memory()
+        h_msg.copy_(self.msg.cpu())
+        h_cw = torch.empty((F, g.words(c.n())), dtype=torch.int64, pin_memory=True)
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())
+
+        def host_step():
+            C.check(C.lib.gf2c_encode_batch(c.handle, vp(h_msg), F, vp(h_cw), C.MEM_HOST, None))
+        return host_step, F * g.words(c.k()) * 8, F * g.words(c.n()) * 8
+
+
+def run_cpu_enc(steps, warmup, cores=None):
+    """The oracle's systematic encoder (same unique codeword as the reference's
+    RuEncodingMatrices::encode) on a sample of messages of the enc workload's
+    code, chunks encoded concurrently on all host threads."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+
+    from oracle import pyoracle
+    pyoracle.build()
+    cores = cores or os.cpu_count() or 1
+    code = pyoracle.Code.dvbt2(0, 1)
+    S = 512 * cores
+    msg = np.random.default_rng(9).integers(0, 2, (S, code.k), dtype=np.uint8)
+    chunks = [c for c in np.array_split(np.arange(S), cores) if len(c)]
+    times = []
+    with ThreadPoolExecutor(cores) as ex:
+        for s in range(warmup + max(steps, 1)):
+            t0 = time.perf_counter()
+            list(ex.map(lambda ix: code.encode(msg[ix[0]:ix[-1] + 1]), chunks))
+            dt = time.perf_counter() - t0
+            if s >= warmup:
+                times.append(dt)
+    tot = sum(times)
+    gbps = S * code.k * len(times) / tot / 1e9
+    sample = (f"{S} messages of the enc workload's code, oracle encoder on {cores} threads, "
+              f"{len(times)} timed passes of {tot / len(times):.2f} s")
+    return gbps, dict(cores=cores, sample=sample, frames=S)
+
+
 def make_workload(name, dev, rank, frames):
     if name in SINGLE:
         return SingleCode(name, dev, rank, frames)
@@ -616,6 +719,8 @@ def make_workload(name, dev, rank, frames):
         return Mixed(dev, rank, frames)
     if name == "bch":
         return BchBatch(dev, rank, frames)
+    if name == "enc":
+        return EncBatch(dev, rank, frames)
     return LearnedScale(dev, rank, frames)
 
 
@@ -631,14 +736,17 @@ def main():
         if args.workload == "bch":
             gbps, info = run_cpu_bch(args.steps, args.warmup)
             desc, decoder, metric = BCH_DESC, "reference BchDecoder::decode (CPU restatement)", BCH_METRIC
+        elif args.workload == "enc":
+            gbps, info = run_cpu_enc(args.steps, args.warmup)
+            desc, decoder, metric = ENC_DESC, "reference systematic LDPC encoder (CPU restatement)", ENC_METRIC
         else:
             gbps, info = run_cpu_reference(args.workload, 1, args.steps, args.warmup)
             desc = SINGLE[args.workload]["desc"] if args.workload in SINGLE else args.workload
             decoder, metric = "reference flooding min-sum (CPU restatement)", METRIC
         line = {"metric": metric, "value": gbps, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "u16" if args.workload == "bch" else "f32",
-                "data": BCH_DATA if args.workload == "bch" else "synthetic (seeded Philox AWGN frames)",
+                "vs_baseline": None, "dtype": {"bch": "u16", "enc": "u32"}.get(args.workload, "f32"),
+                "data": data_of(args.workload, False),
                 "config": {"workload": desc, "decoder": decoder},
                 "cpu_baseline": {"value": gbps, "unit": UNIT, "cores": info["cores"], "kind": "port",
                                  "sample": info["sample"]},
@@ -719,6 +827,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         if args.workload == "bch":
             gbps, info = run_cpu_bch(1, 0)
+        elif args.workload == "enc":
+            gbps, info = run_cpu_enc(1, 0)
         else:
             gbps, info = run_cpu_reference(args.workload, 1, 1, 0)
         cpu = {"value": gbps, "unit": UNIT, "cores": info["cores"], "kind": "port", "sample": info["sample"]}
@@ -727,11 +837,11 @@ def main():
         config = {"workload": wl.desc, "frames_per_gpu": getattr(wl, "frames", None),
                   "l2": "inputs larger than L2 (no flush)",
                   "parallelism": f"replicas x{world} (frames sharded by index, no data-path collective)"}
-        line = {"metric": BCH_METRIC if args.workload == "bch" else METRIC, "value": value, "unit": UNIT,
+        line = {"metric": metric_of(args.workload), "value": value, "unit": UNIT,
                 "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype,
-                "data": BCH_DATA if args.workload == "bch" else "synthetic (seeded Philox AWGN frames, BPSK, encoder output)",
+                "data": data_of(args.workload, True),
                 "config": config,
                 "iterations": iters,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
