@@ -61,6 +61,7 @@ struct gf2c_decoder {
   DevBuf d_codes;
   int max_n = 0, max_m = 0, max_words_k = 0, max_e_slots = 0, max_dc = 0, max_nchk = 0;
   int dcmax = 0, threads = 0, grid = 0, bitmap_words = 0, parity_words = 0, smem_app_floats = 0;
+  int lay_dbuf_off = 0, lay_dbuf_floats = 0;
   const void* kernel = nullptr;
   bool state_flood = false;  // check-state flooding min-sum kernel (state_flood.cu)
   int sf_app_soff = 0;
@@ -352,6 +353,17 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   for (auto* c : d->codes)
     if (smem_of((int)c->h->n) <= (size_t)kSmemBudget) d->smem_app_floats = std::max(d->smem_app_floats, (int)c->h->n);
   d->smem = smem_of(d->smem_app_floats);
+  if (layered && o.algorithm == GF2C_ALGO_SPA_FAST) {
+    // row groups with repeated variables: old messages / deltas of every slot
+    int fl = 0;
+    for (auto* c : d->codes)
+      for (size_t g = 0; g < c->h->cg.size(); g++)
+        if (c->h->cg_sync[g] != 0) fl = std::max(fl, c->h->cg[g].z * c->h->cg[g].y);
+    if (fl > 0) {  // taken below where it costs no occupancy
+      d->lay_dbuf_off = (int)((d->smem + 15) & ~(size_t)15);
+      d->lay_dbuf_floats = fl;
+    }
+  }
   const size_t msg_bytes = o.msg_dtype == GF2C_MSG_F16 ? 2 : 4;
   const long long c2v_bytes = (((long long)d->max_e_slots * msg_bytes) + 255) / 256 * 256;
   d->app_offset = c2v_bytes;
@@ -405,6 +417,22 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   if (!d->kernel) return set_error(GF2C_ERR_UNSUPPORTED, "no decode kernel for this configuration");
   if (!layered && !d->state_flood && threads > 512)
     return set_error(GF2C_ERR_INVALID_ARG, "flooding schedule: threads_per_block must be <= 512");
+  if (d->lay_dbuf_floats > 0) {
+    int optin = 0, occ0 = 0, occ1 = 0;
+    GF2C_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->dev));
+    const size_t with = (size_t)d->lay_dbuf_off + (size_t)d->lay_dbuf_floats * 4;
+    if (with <= (size_t)optin) {
+      GF2C_CUDA(cudaFuncSetAttribute(d->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)with));
+      GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, d->kernel, threads, d->smem));
+      GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, d->kernel, threads, with));
+    }
+    if (occ1 > 0 && occ1 >= occ0) {
+      d->smem = with;
+    } else {
+      d->lay_dbuf_off = 0;
+      d->lay_dbuf_floats = 0;
+    }
+  }
   GF2C_CUDA(cudaFuncSetAttribute(d->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d->smem));
   int occ = 0;
   GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, d->kernel, threads, d->smem));
@@ -445,6 +473,8 @@ static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaSt
   a.smem_app_floats = d->smem_app_floats;
   a.bitmap_words = d->bitmap_words;
   a.parity_words = d->parity_words;
+  a.lay_dbuf_off = d->lay_dbuf_off;
+  a.lay_dbuf_floats = d->lay_dbuf_floats;
   a.alpha = (const float*)d->alpha.p;
   a.beta = (const float*)d->beta.p;
   a.nms_iters = d->opts.algorithm == GF2C_ALGO_NMS ? d->nms_iters : 0;

@@ -186,6 +186,7 @@ struct DecodeArgs {
   int smem_app_floats;             // APP kept in shared memory when n <= this
   int bitmap_words;                // 32-bit words of the hard-decision bitmap
   int parity_words;                // 32-bit words of the check-parity bitmap (layered)
+  int lay_dbuf_off, lay_dbuf_floats;  // layered SPA_FAST: shared-memory buffer of slots x checks
   const float* alpha;              // NMS weights [nms_iters][nms_L]
   const float* beta;
   int nms_iters;

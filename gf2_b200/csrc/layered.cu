@@ -82,6 +82,7 @@ struct LayerSmem {
   uint32_t* bitmap;   // hard decisions, n bits
   uint32_t* chkpar;   // parity of each (flattened) check, m bits
   int* unsat;         // number of unsatisfied checks
+  float* dbuf;        // slots x checks of a row group: old messages / deltas (nullptr: none)
 };
 
 // u-order variable of slot descriptor D = {start, wrap} for check t of a row
@@ -164,6 +165,81 @@ __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t,
   }
 }
 
+// Fast sum-product update of check t of a row group with repeated variables
+// (an info block holding several circulants: runs of consecutive slots of the
+// same block, marked by the sync bits).  Phase A: the same check node as
+// spa_fast_row; dbuf[i * nchk + t] receives the old message, then the delta
+// c2v_new - c2v_old; slots outside the runs update their (unique) variable
+// now, APP_old + delta.  Phase B, after a barrier: the thread of the first
+// slot of each run adds the run's deltas to its variable in slot order
+// (ascending circulant shift).  The result is the one of the slot-by-slot
+// update with a barrier between the slots of a block, with one barrier.
+template <int MSG16, int D>
+__device__ __forceinline__ void spa_fast_rep_a(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
+                                               typename MsgIO<MSG16>::T* __restrict__ c2v, bool first,
+                                               uint32_t sync, float* dbuf, const LayerSmem& S,
+                                               const int2* __restrict__ vg, const int* __restrict__ ci, int vgs) {
+  typedef MsgIO<MSG16> IO;
+  const uint32_t rep = sync | (sync << 1);  // slots inside a run
+  float x[D], e[D];
+#pragma unroll
+  for (int i = 0; i < D; i++) x[i] = app[slot_u(__ldg(&sd[i]), t, nchk)];
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    const float o = first ? 0.0f : ld_msg<MSG16>(c2v, s0 + i * nchk);
+    dbuf[i * nchk + t] = o;
+    if (!first) x[i] = __fsub_rn(x[i], o);
+  }
+  uint32_t neg = 0;
+  float N = 1.0f, Dp = 1.0f;
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    neg |= (uint32_t)(x[i] < 0.0f) << i;
+    e[i] = ex2_approx(fabsf(x[i]) * -1.4426950408889634f);
+    N *= fmaxf(1.0f - e[i], 5.9604645e-08f);
+    Dp = __fmaf_rn(Dp, e[i], Dp);
+  }
+  const uint32_t negp = __popc(neg) & 1u;
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    const float ni = fmaxf(1.0f - e[i], 5.9604645e-08f), di = 1.0f + e[i];
+    const float num = __fmaf_rn(Dp, ni, N * di);
+    const float den = fmaxf(__fmaf_rn(Dp, ni, -N * di), num * 5.9604645e-08f);
+    const float mag = fminf(0.69314718055994531f * lg2_approx(num * rcp_approx(den)), 16.635532f);
+    const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
+    st_msg<MSG16>(c2v, s0 + i * nchk, out);
+    const float delta = out - dbuf[i * nchk + t];
+    if ((rep >> i) & 1u) {
+      dbuf[i * nchk + t] = delta;
+    } else {
+      const int v = slot_u(__ldg(&sd[i]), t, nchk);
+      const float ov = app[v];
+      app_put(app, v, ov < 0.0f, __fadd_rn(ov, delta), S, vg, ci, vgs);
+    }
+  }
+}
+
+template <int D>
+__device__ __forceinline__ void spa_fast_rep_b(const int2* __restrict__ sd, int t, int nchk, float* app,
+                                               uint32_t sync, const float* dbuf, const LayerSmem& S,
+                                               const int2* __restrict__ vg, const int* __restrict__ ci, int vgs) {
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    const bool head = ((sync >> i) & 1u) && !(i > 0 && ((sync >> (i - 1)) & 1u));
+    if (head) {
+      const int v = slot_u(__ldg(&sd[i]), t, nchk);
+      const float ov = app[v];
+      float nw = __fadd_rn(ov, dbuf[i * nchk + t]);
+      for (int j = i + 1; j < D && ((sync >> (j - 1)) & 1u); j++) {
+        int tj = v - __ldg(&sd[j]).x;  // the check of slot j that holds v
+        if (tj < 0) tj += nchk;
+        nw = __fadd_rn(nw, dbuf[j * nchk + tj]);
+      }
+      app_put(app, v, ov < 0.0f, nw, S, vg, ci, vgs);
+    }
+  }
+}
+
 // Iterations of one frame with row groups of at most DCMAX slots; returns the
 // iteration count and whether the syndrome test passed at an early stop.
 template <int ALGO, int MSG16, int DCMAX>
@@ -196,7 +272,14 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
       float ap[DCMAX], o[DCMAX], w[DCMAX];
       uint32_t real = 0, neg = 0, apneg = 0;
       const uint32_t ab = (act && t == 0) ? __ldg(&absent[g]) : 0u;
-      if (ALGO == L_SPA_FAST && DCMAX <= 16 && act && sync == 0 && d == DCMAX && ab == 0) {
+      // row group with repeated variables, all slots real everywhere: one barrier
+      const bool rep_row = ALGO == L_SPA_FAST && DCMAX <= 16 && S.dbuf != nullptr && sync != 0 && d == DCMAX &&
+                           __ldg(&absent[g]) == 0u;
+      if (rep_row) {
+        if (act) spa_fast_rep_a<MSG16, DCMAX>(sd, t, nchk, s0, app, c2v, first, sync, S.dbuf, S, vg, vg_chk, vgs);
+        __syncthreads();
+        if (act) spa_fast_rep_b<DCMAX>(sd, t, nchk, app, sync, S.dbuf, S, vg, vg_chk, vgs);
+      } else if (ALGO == L_SPA_FAST && DCMAX <= 16 && act && sync == 0 && d == DCMAX && ab == 0) {
         spa_fast_row<MSG16, DCMAX>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs);
       } else if (act) {
         // 1. indices, 2. all loads, 3. arithmetic
@@ -303,7 +386,7 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
           }
         }
       }
-      if (sync != 0) {
+      if (sync != 0 && !rep_row) {
         __syncthreads();  // all pre-layer APP reads done
 #pragma unroll
         for (int i = 0; i < DCMAX; i++) {
@@ -345,7 +428,7 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
   MsgT* __restrict__ c2v = (MsgT*)work;
   float* gapp = (float*)(work + a.app_offset);
   const int tid = threadIdx.x, NT = blockDim.x;
-  LayerSmem S{bitmap, chkpar, &s_unsat};
+  LayerSmem S{bitmap, chkpar, &s_unsat, a.lay_dbuf_floats ? (float*)(smem_raw + a.lay_dbuf_off) : nullptr};
 
   for (;;) {
     if (tid == 0) {

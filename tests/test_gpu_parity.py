@@ -107,10 +107,13 @@ def test_layered_dup_blocks_parity(gpu, oracle, idx):
         assert_same_decode(r, ocode.decode(llr, 20, algo=oalgo, sched=1, msg16=True), code.k())
 
 
-@pytest.mark.parametrize("idx,sched,msg16,ebn0", [(6, 1, True, 1.1), (1, 1, True, 1.2), (6, 0, False, 1.1)])
+@pytest.mark.parametrize("idx,sched,msg16,ebn0", [(6, 1, True, 1.1), (1, 1, True, 1.2), (5, 1, False, 3.3),
+                                                  (6, 0, False, 1.1)])
 def test_spa_fast_against_fp64(gpu, oracle, idx, sched, msg16, ebn0):
     """SFU sum-product: not bit-exact; judged against the FP64 sum-product oracle
-    (same schedule) by frame errors and by the deviation of the posteriors."""
+    (same schedule) by frame errors and by the deviation of the posteriors.
+    Normal 3/5 and 5/6 (layered) hold row groups with up to 3 and 4 circulants
+    in one block: the one-barrier path for repeated variables."""
     code = dvb(idx)
     ocode = oracle.Code.dvbt2(idx // 6, idx % 6)
     info, _, llr = ocode.channel(21, 0, 48, ebn0)
