@@ -76,14 +76,24 @@ struct gf2c_decoder {
   std::map<GraphKey, cudaGraphExec_t> graphs;
   cudaStream_t gstream = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // pipelined host-memory batches: a second stream with its own workspace and queue
+  cudaStream_t pstream = nullptr;
+  cudaEvent_t pev_fork = nullptr, pev_join = nullptr, pev_copy[2] = {nullptr, nullptr};
+  DevBuf work2, queue2;
   ~gf2c_decoder() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     if (gstream) {
       cudaStreamSynchronize(gstream);
       cudaStreamDestroy(gstream);
     }
+    if (pstream) {
+      cudaStreamSynchronize(pstream);
+      cudaStreamDestroy(pstream);
+    }
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
+    for (cudaEvent_t e : {pev_fork, pev_join, pev_copy[0], pev_copy[1]})
+      if (e) cudaEventDestroy(e);
   }
 };
 
@@ -462,12 +472,13 @@ int gf2c_decoder_last_launches(const gf2c_decoder* dec, int32_t* launches) {
   return GF2C_OK;
 }
 
-static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaStream_t st) {
+// slot 1: the second workspace and queue of the pipelined host-memory path
+static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaStream_t st, int slot = 0) {
   a.codes = (const DevCode*)d->d_codes.p;
   a.ncodes = (int)d->codes.size();
   a.frames = frames;
-  a.queue = (unsigned long long*)d->queue.p;
-  a.work = (char*)d->work.p;
+  a.queue = (unsigned long long*)(slot ? d->queue2.p : d->queue.p);
+  a.work = (char*)(slot ? d->work2.p : d->work.p);
   a.work_stride = d->work_stride;
   a.app_offset = d->app_offset;
   a.smem_app_floats = d->smem_app_floats;
@@ -486,7 +497,7 @@ static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaSt
   a.sf_llr_off = d->sf_llr_off;
   a.sf_st_off = d->sf_st_off;
   a.sf_app_off = d->sf_app_off;
-  GF2C_CUDA(cudaMemsetAsync(d->queue.p, 0, sizeof(unsigned long long), st));
+  GF2C_CUDA(cudaMemsetAsync(a.queue, 0, sizeof(unsigned long long), st));
   int grid = (int)std::min<int64_t>(d->grid, frames);
   d->last_launches = 1;
   void* args[] = {(void*)&a};
@@ -503,6 +514,28 @@ static int check_status(gf2c_decoder* d, cudaStream_t st) {
     return set_error(GF2C_ERR_INVALID_ARG, "a frame referenced a code id outside the decoder's codes");
   }
   return GF2C_OK;
+}
+
+// The second stream, workspace and queue of the pipelined host-memory path
+// (made on first use; false where they cannot be had, and the call then runs
+// unpipelined).
+static bool pipeline_ready(gf2c_decoder* d) {
+  if (!d->pstream && cudaStreamCreateWithFlags(&d->pstream, cudaStreamNonBlocking) != cudaSuccess) {
+    d->pstream = nullptr;
+    cudaGetLastError();
+    return false;
+  }
+  for (cudaEvent_t* e : {&d->pev_fork, &d->pev_join, &d->pev_copy[0], &d->pev_copy[1]})
+    if (!*e && cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) {
+      *e = nullptr;
+      cudaGetLastError();
+      return false;
+    }
+  if (d->work2.ensure((size_t)d->work_stride * d->grid) != GF2C_OK || d->queue2.ensure(64) != GF2C_OK) {
+    cudaGetLastError();  // an allocation failure: the call runs unpipelined
+    return false;
+  }
+  return true;
 }
 
 int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32_t max_iter, uint64_t* msg_bits,
@@ -531,6 +564,50 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
       (rc = dec->s_cv.ensure(frames)) || (rc = dec->s_so.ensure(frames)))
     return rc;
   if (beliefs && (rc = dec->s_bel.ensure(bl))) return rc;
+  // Large batches: chunks of frames alternating between the caller's stream and
+  // a second stream, each stream running copy in, decode and copy out of its
+  // chunks in order.  Copies overlap the decode of the other stream's chunk,
+  // and a chunk's decode starts on the SMs that the previous chunk's last
+  // frames leave free (each stream has its own workspace and frame queue).
+  const int64_t chunk = std::max<int64_t>(dec->grid, (frames + 7) / 8);
+  if (frames >= 2 * chunk && bl >= ((size_t)64 << 20) && pipeline_ready(dec)) {
+    GF2C_CUDA(cudaEventRecord(dec->pev_fork, st));
+    GF2C_CUDA(cudaStreamWaitEvent(dec->pstream, dec->pev_fork, 0));
+    int chunks = 0;
+    for (int64_t f0 = 0; f0 < frames; f0 += chunk, chunks++) {
+      const int64_t nf = std::min(chunk, frames - f0);
+      const int slot = chunks & 1;
+      cudaStream_t s = slot ? dec->pstream : st;
+      const size_t ln = (size_t)nf * h.n * 4, lo = (size_t)f0 * h.n * 4;
+      const size_t mn = (size_t)nf * wk * 8, mo = (size_t)f0 * wk * 8;
+      // input copies in chunk order, one at a time (the first decode waits for the first copy only)
+      if (chunks > 0) GF2C_CUDA(cudaStreamWaitEvent(s, dec->pev_copy[slot ^ 1], 0));
+      GF2C_CUDA(cudaMemcpyAsync((char*)dec->s_llr.p + lo, (const char*)llr + lo, ln, cudaMemcpyHostToDevice, s));
+      GF2C_CUDA(cudaEventRecord(dec->pev_copy[slot], s));
+      DecodeArgs b = a;
+      b.llr = (const float*)((char*)dec->s_llr.p + lo);
+      b.msg = msg_bits ? (uint64_t*)((char*)dec->s_msg.p + mo) : nullptr;
+      b.iters = (int32_t*)dec->s_it.p + f0;
+      b.conv = (uint8_t*)dec->s_cv.p + f0;
+      b.synd_ok = (uint8_t*)dec->s_so.p + f0;
+      b.beliefs = beliefs ? (float*)((char*)dec->s_bel.p + lo) : nullptr;
+      if ((rc = launch_decoder(dec, b, nf, s, slot))) return rc;
+      if (msg_bits)
+        GF2C_CUDA(cudaMemcpyAsync((char*)msg_bits + mo, (char*)dec->s_msg.p + mo, mn, cudaMemcpyDeviceToHost, s));
+      if (iterations)
+        GF2C_CUDA(cudaMemcpyAsync(iterations + f0, (int32_t*)dec->s_it.p + f0, nf * 4, cudaMemcpyDeviceToHost, s));
+      if (converged)
+        GF2C_CUDA(cudaMemcpyAsync(converged + f0, (uint8_t*)dec->s_cv.p + f0, nf, cudaMemcpyDeviceToHost, s));
+      if (syndrome_ok)
+        GF2C_CUDA(cudaMemcpyAsync(syndrome_ok + f0, (uint8_t*)dec->s_so.p + f0, nf, cudaMemcpyDeviceToHost, s));
+      if (beliefs)
+        GF2C_CUDA(cudaMemcpyAsync((char*)beliefs + lo, (char*)dec->s_bel.p + lo, ln, cudaMemcpyDeviceToHost, s));
+    }
+    GF2C_CUDA(cudaEventRecord(dec->pev_join, dec->pstream));
+    GF2C_CUDA(cudaStreamWaitEvent(st, dec->pev_join, 0));
+    dec->last_launches = chunks;
+    return check_status(dec, st);
+  }
   GF2C_CUDA(cudaMemcpyAsync(dec->s_llr.p, llr, bl, cudaMemcpyHostToDevice, st));
   a.llr = (const float*)dec->s_llr.p;
   a.msg = msg_bits ? (uint64_t*)dec->s_msg.p : nullptr;

@@ -26,6 +26,10 @@
  *     GF2C_MEM_HOST (pageable or pinned host memory; the library stages the
  *     copies on `stream`) or GF2C_MEM_DEVICE (device pointers on the current
  *     device).  `stream` is a cudaStream_t (NULL = legacy default stream).
+ *     gf2c_decode_batch splits host-memory batches of 64 MB of LLRs and more
+ *     into chunks that alternate between `stream` and a second stream of the
+ *     decoder (its own workspace), so that copies overlap decoding; pinned
+ *     host memory lets the copies run asynchronously.
  *     Host-memory calls return after the results are in host memory;
  *     device-memory calls are asynchronous on `stream`.
  *   - Code handles are immutable after creation and may be shared by threads.

@@ -197,6 +197,29 @@ def test_device_tensor_path_matches_host(gpu, oracle):
     assert dec.last_launches() == 1
 
 
+@pytest.mark.parametrize("kw", [dict(), dict(algorithm=g.ALGO_SPA_FAST, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16)])
+def test_pipelined_host_path_matches_device(gpu, kw):
+    """Host-memory batches of 64 MB and more run in chunks on two streams (copies
+    overlapping the decode): every output equals the one-launch device path."""
+    import torch
+    code = g.LdpcCode.dvb_t2_short(g.CodeRate.Rate3_5)
+    F = 2048  # 133 MB of LLRs
+    pts = [0.8 + 0.1 * i for i in range(9)]
+    s2 = np.array([g.sigma2_from_ebn0(pts[f % 9], code.rate()) for f in range(F)])
+    _, _, llr = g.awgn_frames(code, 5, 0, F, s2, device=gpu, want_info=False, want_cw=False)
+    dec = g.LdpcDecoder(code, **kw)
+    d = dec.decode_tensors(llr, 30, beliefs=True)
+    torch.cuda.synchronize()
+    assert dec.last_launches() == 1
+    h = dec.decode_arrays(llr.cpu().numpy(), 30, beliefs=True)
+    assert dec.last_launches() > 1
+    assert (d["msg"].cpu().numpy().view(np.uint64) == h["msg"]).all()
+    assert (d["iters"].cpu().numpy() == h["iters"]).all()
+    assert (d["conv"].cpu().numpy() == h["conv"]).all()
+    assert (d["beliefs"].cpu().numpy().view(np.uint32) == h["beliefs"].view(np.uint32)).all()
+    assert 0 < int(h["conv"].sum()) < F
+
+
 @pytest.mark.parametrize("idx", range(12))
 def test_encoder_syndrome_parity(gpu, oracle, idx):
     code = dvb(idx)
