@@ -273,13 +273,13 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
       uint32_t real = 0, neg = 0, apneg = 0;
       const uint32_t ab = (act && t == 0) ? __ldg(&absent[g]) : 0u;
       // row group with repeated variables, all slots real everywhere: one barrier
-      const bool rep_row = ALGO == L_SPA_FAST && DCMAX <= 16 && S.dbuf != nullptr && sync != 0 && d == DCMAX &&
+      const bool rep_row = ALGO == L_SPA_FAST && DCMAX <= 22 && S.dbuf != nullptr && sync != 0 && d == DCMAX &&
                            __ldg(&absent[g]) == 0u;
       if (rep_row) {
         if (act) spa_fast_rep_a<MSG16, DCMAX>(sd, t, nchk, s0, app, c2v, first, sync, S.dbuf, S, vg, vg_chk, vgs);
         __syncthreads();
         if (act) spa_fast_rep_b<DCMAX>(sd, t, nchk, app, sync, S.dbuf, S, vg, vg_chk, vgs);
-      } else if (ALGO == L_SPA_FAST && DCMAX <= 16 && act && sync == 0 && d == DCMAX && ab == 0) {
+      } else if (ALGO == L_SPA_FAST && DCMAX <= 22 && act && sync == 0 && d == DCMAX && ab == 0) {
         spa_fast_row<MSG16, DCMAX>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs);
       } else if (act) {
         // 1. indices, 2. all loads, 3. arithmetic
