@@ -119,22 +119,25 @@ __device__ __forceinline__ void app_put(float* app, int v, bool old_neg, float n
 // edge and whose variables are all distinct (the common case): loads, check
 // node, message stores and posterior updates in one pass; flipped hard
 // decisions are collected in a mask and handled after the loop (one call
-// site).  Same arithmetic as the general path of bp_layered_kernel.
-template <int MSG16, int D>
+// site).  Same arithmetic as the general path of bp_layered_kernel.  PART:
+// the row group has d < D slots; slots d..D-1 take a neutral input (e = 0,
+// positive, as the general path's missing edges) and store nothing.
+template <int MSG16, int D, bool PART>
 __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
                                              typename MsgIO<MSG16>::T* __restrict__ c2v, bool first,
                                              const LayerSmem& S, const int2* __restrict__ vg,
-                                             const int* __restrict__ ci, int vgs) {
+                                             const int* __restrict__ ci, int vgs, int d) {
   typedef MsgIO<MSG16> IO;
   float x[D], e[D];
 #pragma unroll
-  for (int i = 0; i < D; i++) x[i] = app[slot_u(__ldg(&sd[i]), t, nchk)];
+  for (int i = 0; i < D; i++) x[i] = (!PART || i < d) ? app[slot_u(__ldg(&sd[i]), t, nchk)] : 3.402823466e38f;
   uint32_t neg = 0, apneg = 0;
 #pragma unroll
   for (int i = 0; i < D; i++) apneg |= (uint32_t)(x[i] < 0.0f) << i;
   if (!first) {
 #pragma unroll
-    for (int i = 0; i < D; i++) x[i] = __fsub_rn(x[i], ld_msg<MSG16>(c2v, s0 + i * nchk));
+    for (int i = 0; i < D; i++)
+      if (!PART || i < d) x[i] = __fsub_rn(x[i], ld_msg<MSG16>(c2v, s0 + i * nchk));
   }
   float N = 1.0f, Dp = 1.0f;
 #pragma unroll
@@ -152,11 +155,13 @@ __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t,
     const float num = __fmaf_rn(Dp, ni, N * di);
     const float den = fmaxf(__fmaf_rn(Dp, ni, -N * di), num * 5.9604645e-08f);
     const float mag = fminf(0.69314718055994531f * lg2_approx(num * rcp_approx(den)), 16.635532f);
-    const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
-    st_msg<MSG16>(c2v, s0 + i * nchk, out);
-    const float nw = x[i] + out;
-    app[slot_u(__ldg(&sd[i]), t, nchk)] = nw;
-    flips |= (uint32_t)(((apneg >> i) & 1u) != (uint32_t)(nw < 0.0f)) << i;
+    if (!PART || i < d) {
+      const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
+      st_msg<MSG16>(c2v, s0 + i * nchk, out);
+      const float nw = x[i] + out;
+      app[slot_u(__ldg(&sd[i]), t, nchk)] = nw;
+      flips |= (uint32_t)(((apneg >> i) & 1u) != (uint32_t)(nw < 0.0f)) << i;
+    }
   }
   while (flips) {  // rare after the first iterations
     const int i = __ffs(flips) - 1;
@@ -174,21 +179,24 @@ __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t,
 // slot of each run adds the run's deltas to its variable in slot order
 // (ascending circulant shift).  The result is the one of the slot-by-slot
 // update with a barrier between the slots of a block, with one barrier.
-template <int MSG16, int D>
+template <int MSG16, int D, bool PART>
 __device__ __forceinline__ void spa_fast_rep_a(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
                                                typename MsgIO<MSG16>::T* __restrict__ c2v, bool first,
                                                uint32_t sync, float* dbuf, const LayerSmem& S,
-                                               const int2* __restrict__ vg, const int* __restrict__ ci, int vgs) {
+                                               const int2* __restrict__ vg, const int* __restrict__ ci, int vgs,
+                                               int d) {
   typedef MsgIO<MSG16> IO;
   const uint32_t rep = sync | (sync << 1);  // slots inside a run
   float x[D], e[D];
 #pragma unroll
-  for (int i = 0; i < D; i++) x[i] = app[slot_u(__ldg(&sd[i]), t, nchk)];
+  for (int i = 0; i < D; i++) x[i] = (!PART || i < d) ? app[slot_u(__ldg(&sd[i]), t, nchk)] : 3.402823466e38f;
 #pragma unroll
   for (int i = 0; i < D; i++) {
-    const float o = first ? 0.0f : ld_msg<MSG16>(c2v, s0 + i * nchk);
-    dbuf[i * nchk + t] = o;
-    if (!first) x[i] = __fsub_rn(x[i], o);
+    if (!PART || i < d) {
+      const float o = first ? 0.0f : ld_msg<MSG16>(c2v, s0 + i * nchk);
+      dbuf[i * nchk + t] = o;
+      if (!first) x[i] = __fsub_rn(x[i], o);
+    }
   }
   uint32_t neg = 0;
   float N = 1.0f, Dp = 1.0f;
@@ -206,15 +214,17 @@ __device__ __forceinline__ void spa_fast_rep_a(const int2* __restrict__ sd, int 
     const float num = __fmaf_rn(Dp, ni, N * di);
     const float den = fmaxf(__fmaf_rn(Dp, ni, -N * di), num * 5.9604645e-08f);
     const float mag = fminf(0.69314718055994531f * lg2_approx(num * rcp_approx(den)), 16.635532f);
-    const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
-    st_msg<MSG16>(c2v, s0 + i * nchk, out);
-    const float delta = out - dbuf[i * nchk + t];
-    if ((rep >> i) & 1u) {
-      dbuf[i * nchk + t] = delta;
-    } else {
-      const int v = slot_u(__ldg(&sd[i]), t, nchk);
-      const float ov = app[v];
-      app_put(app, v, ov < 0.0f, __fadd_rn(ov, delta), S, vg, ci, vgs);
+    if (!PART || i < d) {
+      const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
+      st_msg<MSG16>(c2v, s0 + i * nchk, out);
+      const float delta = out - dbuf[i * nchk + t];
+      if ((rep >> i) & 1u) {
+        dbuf[i * nchk + t] = delta;
+      } else {
+        const int v = slot_u(__ldg(&sd[i]), t, nchk);
+        const float ov = app[v];
+        app_put(app, v, ov < 0.0f, __fadd_rn(ov, delta), S, vg, ci, vgs);
+      }
     }
   }
 }
@@ -273,14 +283,23 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
       uint32_t real = 0, neg = 0, apneg = 0;
       const uint32_t ab = (act && t == 0) ? __ldg(&absent[g]) : 0u;
       // row group with repeated variables, all slots real everywhere: one barrier
-      const bool rep_row = ALGO == L_SPA_FAST && DCMAX <= 22 && S.dbuf != nullptr && sync != 0 && d == DCMAX &&
-                           __ldg(&absent[g]) == 0u;
+      // (fewer slots than DCMAX: the PART variants)
+      const bool rep_row = ALGO == L_SPA_FAST && DCMAX <= 22 && S.dbuf != nullptr && sync != 0 && d >= 2 &&
+                           d <= DCMAX && __ldg(&absent[g]) == 0u;
       if (rep_row) {
-        if (act) spa_fast_rep_a<MSG16, DCMAX>(sd, t, nchk, s0, app, c2v, first, sync, S.dbuf, S, vg, vg_chk, vgs);
+        if (act) {
+          if (d == DCMAX)
+            spa_fast_rep_a<MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, first, sync, S.dbuf, S, vg, vg_chk, vgs, d);
+          else
+            spa_fast_rep_a<MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, first, sync, S.dbuf, S, vg, vg_chk, vgs, d);
+        }
         __syncthreads();
         if (act) spa_fast_rep_b<DCMAX>(sd, t, nchk, app, sync, S.dbuf, S, vg, vg_chk, vgs);
-      } else if (ALGO == L_SPA_FAST && DCMAX <= 22 && act && sync == 0 && d == DCMAX && ab == 0) {
-        spa_fast_row<MSG16, DCMAX>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs);
+      } else if (ALGO == L_SPA_FAST && DCMAX <= 22 && act && sync == 0 && d >= 2 && d <= DCMAX && ab == 0) {
+        if (d == DCMAX)
+          spa_fast_row<MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs, d);
+        else
+          spa_fast_row<MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs, d);
       } else if (act) {
         // 1. indices, 2. all loads, 3. arithmetic
 #pragma unroll
