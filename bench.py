@@ -345,7 +345,8 @@ class Mixed:
                                  msg_dtype=self.msg16, threads_per_block=threads, blocks_per_sm=bps)
         self.desc = (f"mixed batch: {self.frames} frames uniform over the 12 DVB-T2 codes, per-frame Eb/N0 "
                      f"U[thr, thr+1] (thr = shannon_limit(k/n)), per-frame budget U{{10..50}}, layered "
-                     f"sum-product (SFU) fp16, one persistent launch from a CUDA graph, autotuned shape "
+                     f"sum-product (SFU) fp16, an ordering kernel (frames grouped by code) and one persistent decode launch "
+                     f"from a CUDA graph, autotuned shape "
                      f"threads={threads} blocks/SM={bps or 'max'}")
         self.dtype = "f32"
 

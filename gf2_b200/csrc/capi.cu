@@ -80,6 +80,8 @@ struct gf2c_decoder {
   cudaStream_t pstream = nullptr;
   cudaEvent_t pev_fork = nullptr, pev_join = nullptr, pev_copy[2] = {nullptr, nullptr};
   DevBuf work2, queue2;
+  // mixed batches: rank of each code in the frame order (longest codes first), frame order buffer
+  DevBuf d_rank, d_order;
   ~gf2c_decoder() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     if (gstream) {
@@ -326,6 +328,16 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   int rc = d->d_codes.ensure(sizeof(DevCode) * dc.size());
   if (rc) return rc;
   GF2C_CUDA(cudaMemcpy(d->d_codes.p, dc.data(), sizeof(DevCode) * dc.size(), cudaMemcpyHostToDevice));
+  if (d->codes.size() > 1) {
+    // mixed batches are decoded code by code: longest frames first, then by code index
+    std::vector<int> by(d->codes.size());
+    for (size_t i = 0; i < by.size(); i++) by[i] = (int)i;
+    std::stable_sort(by.begin(), by.end(), [&](int x, int y) { return d->codes[x]->h->n > d->codes[y]->h->n; });
+    std::vector<int32_t> rank(by.size());
+    for (size_t r = 0; r < by.size(); r++) rank[by[r]] = (int32_t)r;
+    if ((rc = d->d_rank.ensure(sizeof(int32_t) * rank.size()))) return rc;
+    GF2C_CUDA(cudaMemcpy(d->d_rank.p, rank.data(), sizeof(int32_t) * rank.size(), cudaMemcpyHostToDevice));
+  }
 
   // NMS weights
   if (o.algorithm == GF2C_ALGO_NMS) {
@@ -635,6 +647,28 @@ int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_of
   if (rc || frames == 0) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   DecodeArgs a{};
+  // Frames of a mixed batch are taken code by code (the ordering kernel runs
+  // before the decode, in the same stream or graph).  A larger order buffer
+  // invalidates the graphs that captured the old one.
+  const bool ordered = dec->codes.size() > 1;
+  if (ordered) {
+    void* before = dec->d_order.p;
+    if ((rc = dec->d_order.ensure((size_t)frames * 8))) return rc;
+    if (dec->d_order.p != before && !dec->graphs.empty()) {
+      if (dec->gstream) GF2C_CUDA(cudaStreamSynchronize(dec->gstream));
+      for (auto& kv : dec->graphs) cudaGraphExecDestroy(kv.second);
+      dec->graphs.clear();
+    }
+    a.order = (const int64_t*)dec->d_order.p;
+  }
+  auto order_then_decode = [&](cudaStream_t s) -> int {
+    if (ordered)
+      GF2C_CUDA(launch_mixed_order(a.code_id, frames, (const int32_t*)dec->d_rank.p, (int)dec->codes.size(),
+                                   (int64_t*)dec->d_order.p, s));
+    int r = launch_decoder(dec, a, frames, s);
+    if (!r && ordered) dec->last_launches = 2;
+    return r;
+  };
   if (mem == GF2C_MEM_DEVICE) {
     a.llr = llr;
     a.llr_off = llr_offset;
@@ -645,7 +679,7 @@ int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_of
     a.iters = iterations;
     a.conv = converged;
     a.synd_ok = syndrome_ok;
-    if (!use_graph) return launch_decoder(dec, a, frames, st);
+    if (!use_graph) return order_then_decode(st);
     GraphKey key;
     key.v = {(uintptr_t)llr, (uintptr_t)llr_offset, (uintptr_t)code_id, (uintptr_t)max_iter,
              (uintptr_t)msg_bits, (uintptr_t)msg_offset, (uintptr_t)iterations, (uintptr_t)converged,
@@ -663,7 +697,7 @@ int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_of
     if (it == dec->graphs.end()) {
       cudaGraph_t g;
       GF2C_CUDA(cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal));
-      rc = launch_decoder(dec, a, frames, gs);
+      rc = order_then_decode(gs);
       cudaError_t e = cudaStreamEndCapture(gs, &g);
       if (rc) return rc;
       if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");
@@ -678,7 +712,7 @@ int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_of
     GF2C_CUDA(cudaGraphLaunch(it->second, gs));
     GF2C_CUDA(cudaEventRecord(dec->ev_out, gs));
     GF2C_CUDA(cudaStreamWaitEvent(st, dec->ev_out, 0));
-    dec->last_launches = 1;
+    dec->last_launches = ordered ? 2 : 1;
     return GF2C_OK;
   }
   // host memory: validate ids and offsets, stage everything
@@ -711,7 +745,7 @@ int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_of
   a.iters = (int32_t*)dec->s_it.p;
   a.conv = (uint8_t*)dec->s_cv.p;
   a.synd_ok = (uint8_t*)dec->s_so.p;
-  if ((rc = launch_decoder(dec, a, frames, st))) return rc;
+  if ((rc = order_then_decode(st))) return rc;
   if (msg_bits) GF2C_CUDA(cudaMemcpyAsync(msg_bits, dec->s_msg.p, msg_total * 8, cudaMemcpyDeviceToHost, st));
   if (iterations) GF2C_CUDA(cudaMemcpyAsync(iterations, dec->s_it.p, frames * 4, cudaMemcpyDeviceToHost, st));
   if (converged) GF2C_CUDA(cudaMemcpyAsync(converged, dec->s_cv.p, frames, cudaMemcpyDeviceToHost, st));

@@ -269,7 +269,10 @@ __global__ void __launch_bounds__(512) bp_decode_kernel(const DecodeArgs a) {
   const int tid = threadIdx.x, NT = blockDim.x;
 
   for (;;) {
-    if (tid == 0) s_frame = (long long)atomicAdd(a.queue, 1ull);
+    if (tid == 0) {
+      const long long q = (long long)atomicAdd(a.queue, 1ull);
+      s_frame = (a.order != nullptr && q < a.frames) ? a.order[q] : q;
+    }
     __syncthreads();
     const long long f = s_frame;
     if (f >= a.frames) break;
@@ -405,6 +408,50 @@ static const void* kernel_dc(int dcmax) {
     case 64: return (const void*)bp_decode_kernel<ALGO, MSG16, 64>;
   }
   return nullptr;
+}
+
+// Frame order of a mixed batch: for each rank, a block-wide stable compaction
+// of the frames of that rank (ballot + popc within a warp, warp totals in
+// shared memory).  Decoding the frames of one code together keeps the SMs on
+// one slot count's code path at a time.
+__global__ void __launch_bounds__(1024) mixed_order_kernel(const int32_t* __restrict__ code_id, int64_t frames,
+                                                           const int32_t* __restrict__ rank_of, int ncodes,
+                                                           int64_t* __restrict__ order) {
+  __shared__ int s_warp[32];
+  __shared__ long long s_pos;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  if (tid == 0) s_pos = 0;
+  __syncthreads();
+  for (int r = 0; r <= ncodes; r++) {
+    for (long long base = 0; base < frames; base += blockDim.x) {
+      const long long f = base + tid;
+      bool hit = false;
+      if (f < frames) {
+        const int c = code_id[f];
+        hit = ((c >= 0 && c < ncodes) ? __ldg(&rank_of[c]) : ncodes) == r;
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, hit);
+      if (lane == 0) s_warp[wid] = __popc(b);
+      __syncthreads();
+      int before = 0, total = 0;
+      for (int w = 0; w < nw; w++) {
+        const int x = s_warp[w];
+        before += (w < wid) ? x : 0;
+        total += x;
+      }
+      const long long p0 = s_pos;
+      if (hit) order[p0 + before + __popc(b & ((1u << lane) - 1u))] = f;
+      __syncthreads();  // s_warp and s_pos read by all
+      if (tid == 0) s_pos = p0 + total;
+      __syncthreads();
+    }
+  }
+}
+
+cudaError_t launch_mixed_order(const int32_t* code_id, int64_t frames, const int32_t* rank_of, int ncodes,
+                               int64_t* order, cudaStream_t st) {
+  mixed_order_kernel<<<1, 1024, 0, st>>>(code_id, frames, rank_of, ncodes, order);
+  return cudaGetLastError();
 }
 
 // Flooding-schedule kernel for (algorithm, message type, degree bucket).

@@ -170,6 +170,7 @@ struct DecodeArgs {
   const float* llr;
   const int64_t* llr_off;          // nullable: frame f at f * n
   const int32_t* code_id;          // nullable: code 0
+  const int64_t* order;            // nullable: the queue's q-th frame is order[q] (mixed batches grouped by code)
   const int32_t* max_iter_arr;     // nullable: max_iter for all
   int max_iter;
   uint64_t* msg;
@@ -202,6 +203,10 @@ struct DecodeArgs {
 };
 
 const void* flood_kernel_ptr(int algo, int msg16, int dcmax);
+// Frame order of a mixed batch (one CTA): frames grouped by rank_of[code id],
+// ascending rank, ids outside [0, ncodes) last; ascending frame index within a group.
+cudaError_t launch_mixed_order(const int32_t* code_id, int64_t frames, const int32_t* rank_of, int ncodes,
+                               int64_t* order, cudaStream_t st);
 int state_dcmax_bucket(int max_dc);
 int state_flood_threads();
 const void* state_flood_kernel_ptr(int dcmax, bool all_smem);

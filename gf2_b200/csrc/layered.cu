@@ -451,7 +451,8 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
 
   for (;;) {
     if (tid == 0) {
-      s_frame = (long long)atomicAdd(a.queue, 1ull);
+      const long long q = (long long)atomicAdd(a.queue, 1ull);
+      s_frame = (a.order != nullptr && q < a.frames) ? a.order[q] : q;
       s_unsat = 0;
     }
     __syncthreads();

@@ -249,7 +249,10 @@ __global__ void __launch_bounds__(kStateThreads, 1) bp_state_flood_kernel(const 
   uint4* st = ALL_SMEM ? (uint4*)smem_raw : (uint4*)(work + a.sf_st_off);
   const Post<ALL_SMEM> P{ALL_SMEM ? (float*)(smem_raw + a.sf_app_soff) : (float*)(work + a.sf_app_off)};
   for (;;) {
-    if (tid == 0) s_frame = (long long)atomicAdd(a.queue, 1ull);
+    if (tid == 0) {
+      const long long q = (long long)atomicAdd(a.queue, 1ull);
+      s_frame = (a.order != nullptr && q < a.frames) ? a.order[q] : q;
+    }
     __syncthreads();
     const long long f = s_frame;
     if (f >= a.frames) break;

@@ -177,7 +177,10 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
 /* Mixed batch in one persistent launch: frame f uses code code_id[f] (index into the
  * codes given at creation), reads n[code] LLRs at llr + llr_offset[f], writes
  * ceil(k/64) words at msg_bits + msg_offset[f] (both in elements), and has its own
- * budget max_iter[f].  Per-frame outputs as in gf2c_decode_batch.  With mem ==
+ * budget max_iter[f].  Per-frame outputs as in gf2c_decode_batch.  A decoder of
+ * several codes first runs a small ordering kernel, so that the persistent launch
+ * decodes the frames code by code (longest codes first); a frame's results do not
+ * depend on the order.  With mem ==
  * GF2C_MEM_DEVICE and use_graph = 1 the launch sequence is captured once per
  * (frames, pointers) shape into a CUDA graph and replayed. */
 int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_offset,

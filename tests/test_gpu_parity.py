@@ -357,6 +357,56 @@ def test_mixed_batch_graph_replay(gpu):
         assert (it == 1).all() and cv.all()
 
 
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_mixed_batch_code_order(gpu, use_graph):
+    """Mixed batches are decoded code by code (an ordering kernel before the
+    persistent decode): 2500 frames in random code order and one invalid code
+    id; every frame's results equal a single-code decode of it, the invalid
+    frame reports -1 iterations."""
+    import torch
+    codes = [g.LdpcCode.dvb_t2_short(0), g.LdpcCode.dvb_t2_normal(1), g.LdpcCode.dvb_t2_short(2)]
+    kw = dict(algorithm=g.ALGO_SPA_FAST, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16)
+    dec = g.LdpcDecoder(codes[0], codes=codes, **kw)
+    rng = np.random.default_rng(11)
+    F = 2500
+    cid = rng.choice(3, F, p=[0.45, 0.1, 0.45]).astype(np.int32)
+    budget = [12, 20, 9]
+    mit = np.array([budget[c] for c in cid], np.int32)
+    ebn0 = [1.2, 1.1, 2.2]
+    singles, llr_parts, lo = {}, [], np.zeros(F, np.int64)
+    base = 0
+    for c in range(3):
+        idx = np.nonzero(cid == c)[0]
+        s2 = np.array([g.sigma2_from_ebn0(ebn0[c] + 0.1 * (i % 5), codes[c].rate()) for i in idx])
+        _, _, l = g.awgn_frames(codes[c], 9, c << 20, len(idx), s2, device=gpu, want_info=False, want_cw=False)
+        singles[c] = (idx, g.LdpcDecoder(codes[c], **kw).decode_tensors(l, budget[c]))
+        llr_parts.append(l.reshape(-1))
+        lo[idx] = base + np.arange(len(idx)) * codes[c].n()
+        base += len(idx) * codes[c].n()
+    bad = 7
+    cid_run = cid.copy()
+    cid_run[bad] = 5  # outside the decoder's codes
+    W = max(g.words(c.k()) for c in codes)
+    msg = torch.zeros(F * W, dtype=torch.int64, device=gpu)
+    mo = torch.arange(F, dtype=torch.int64, device=gpu) * W
+    it = torch.zeros(F, dtype=torch.int32, device=gpu)
+    cv = torch.zeros(F, dtype=torch.uint8, device=gpu)
+    so = torch.zeros(F, dtype=torch.uint8, device=gpu)
+    dec.decode_mixed_tensors(torch.cat(llr_parts), torch.from_numpy(lo).to(gpu), torch.from_numpy(cid_run).to(gpu),
+                             torch.from_numpy(mit).to(gpu), msg, mo, it, cv, so, use_graph=use_graph)
+    torch.cuda.synchronize()
+    assert dec.last_launches() == 2
+    itn, cvn, msgn = it.cpu().numpy(), cv.cpu().numpy(), msg.cpu().numpy().view(np.uint64).reshape(F, W)
+    assert itn[bad] == -1
+    for c in range(3):
+        idx, r = singles[c]
+        keep = idx != bad
+        w = g.words(codes[c].k())
+        assert (itn[idx[keep]] == r["iters"].cpu().numpy()[keep]).all()
+        assert (cvn[idx[keep]] == r["conv"].cpu().numpy()[keep]).all()
+        assert (msgn[idx[keep], :w] == r["msg"].cpu().numpy().view(np.uint64)[keep]).all()
+
+
 def test_edge_cases(gpu, oracle):
     # frames == 0 is a no-op; degree-1 check gives a zero message (core.rs:807-811)
     code = g.LdpcCode.from_edges(3, 5, [(0, 0), (1, 1), (1, 2), (2, 2), (2, 3), (2, 4), (1, 4)])
