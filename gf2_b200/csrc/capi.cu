@@ -82,6 +82,8 @@ struct gf2c_decoder {
   DevBuf work2, queue2;
   // mixed batches: rank of each code in the frame order (longest codes first), frame order buffer
   DevBuf d_rank, d_order;
+  // single-code batches, hardest frames first: per-frame keys and order (one pair per stream slot)
+  DevBuf d_key[2], d_korder[2];
   ~gf2c_decoder() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     if (gstream) {
@@ -517,6 +519,32 @@ static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaSt
   return GF2C_OK;
 }
 
+// Single-code batches of more frames than CTAs are decoded hardest frames first
+// (ascending sum of |LLR|), so that the last frames the persistent kernel
+// takes are short ones and the SMs finish together.  Per-frame results do not
+// depend on the order.  Skipped above kKeyOrderMax frames, and while `st` is
+// being captured into a graph if the buffers would have to grow.  Returns the
+// number of kernels launched (0 or 2) in `launches`.
+static int key_order(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaStream_t st, int slot, int& launches) {
+  launches = 0;
+  if (d->codes.size() != 1 || frames <= d->grid || frames > kKeyOrderMax) return GF2C_OK;
+  DevBuf& kb = d->d_key[slot];
+  DevBuf& ob = d->d_korder[slot];
+  if (kb.bytes < (size_t)frames * 4 || ob.bytes < (size_t)frames * 8) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+      cudaGetLastError();
+      return GF2C_OK;
+    }
+    int rc;
+    if ((rc = kb.ensure((size_t)frames * 4)) || (rc = ob.ensure((size_t)frames * 8))) return rc;
+  }
+  GF2C_CUDA(launch_key_order(a.llr, (int)d->codes[0]->h->n, frames, (float*)kb.p, (int64_t*)ob.p, st));
+  a.order = (const int64_t*)ob.p;
+  launches = 2;
+  return GF2C_OK;
+}
+
 static int check_status(gf2c_decoder* d, cudaStream_t st) {
   int h = 0;
   GF2C_CUDA(cudaMemcpyAsync(&h, d->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -568,7 +596,11 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
     a.conv = converged;
     a.synd_ok = syndrome_ok;
     a.beliefs = beliefs;
-    return launch_decoder(dec, a, frames, st);
+    int extra = 0;
+    if ((rc = key_order(dec, a, frames, st, 0, extra))) return rc;
+    if ((rc = launch_decoder(dec, a, frames, st))) return rc;
+    dec->last_launches += extra;
+    return GF2C_OK;
   }
   const int wk = (int)((h.k + 63) / 64);
   size_t bl = (size_t)frames * h.n * 4, bm = (size_t)frames * wk * 8;
@@ -585,7 +617,7 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
   if (frames >= 2 * chunk && bl >= ((size_t)64 << 20) && pipeline_ready(dec)) {
     GF2C_CUDA(cudaEventRecord(dec->pev_fork, st));
     GF2C_CUDA(cudaStreamWaitEvent(dec->pstream, dec->pev_fork, 0));
-    int chunks = 0;
+    int chunks = 0, launches = 0;
     for (int64_t f0 = 0; f0 < frames; f0 += chunk, chunks++) {
       const int64_t nf = std::min(chunk, frames - f0);
       const int slot = chunks & 1;
@@ -603,7 +635,10 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
       b.conv = (uint8_t*)dec->s_cv.p + f0;
       b.synd_ok = (uint8_t*)dec->s_so.p + f0;
       b.beliefs = beliefs ? (float*)((char*)dec->s_bel.p + lo) : nullptr;
+      int extra = 0;
+      if ((rc = key_order(dec, b, nf, s, slot, extra))) return rc;
       if ((rc = launch_decoder(dec, b, nf, s, slot))) return rc;
+      launches += 1 + extra;
       if (msg_bits)
         GF2C_CUDA(cudaMemcpyAsync((char*)msg_bits + mo, (char*)dec->s_msg.p + mo, mn, cudaMemcpyDeviceToHost, s));
       if (iterations)
@@ -617,7 +652,7 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
     }
     GF2C_CUDA(cudaEventRecord(dec->pev_join, dec->pstream));
     GF2C_CUDA(cudaStreamWaitEvent(st, dec->pev_join, 0));
-    dec->last_launches = chunks;
+    dec->last_launches = launches;
     return check_status(dec, st);
   }
   GF2C_CUDA(cudaMemcpyAsync(dec->s_llr.p, llr, bl, cudaMemcpyHostToDevice, st));
@@ -627,7 +662,10 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
   a.conv = (uint8_t*)dec->s_cv.p;
   a.synd_ok = (uint8_t*)dec->s_so.p;
   a.beliefs = beliefs ? (float*)dec->s_bel.p : nullptr;
+  int extra = 0;
+  if ((rc = key_order(dec, a, frames, st, 0, extra))) return rc;
   if ((rc = launch_decoder(dec, a, frames, st))) return rc;
+  dec->last_launches += extra;
   if (msg_bits) GF2C_CUDA(cudaMemcpyAsync(msg_bits, dec->s_msg.p, bm, cudaMemcpyDeviceToHost, st));
   if (iterations) GF2C_CUDA(cudaMemcpyAsync(iterations, dec->s_it.p, frames * 4, cudaMemcpyDeviceToHost, st));
   if (converged) GF2C_CUDA(cudaMemcpyAsync(converged, dec->s_cv.p, frames, cudaMemcpyDeviceToHost, st));

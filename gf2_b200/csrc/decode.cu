@@ -454,6 +454,63 @@ cudaError_t launch_mixed_order(const int32_t* code_id, int64_t frames, const int
   return cudaGetLastError();
 }
 
+// Sum of |LLR| of each frame (one CTA per frame, a fixed summation order).
+__global__ void __launch_bounds__(256) frame_key_kernel(const float* __restrict__ llr, int n,
+                                                        float* __restrict__ key) {
+  __shared__ float s_part[8];
+  const float* __restrict__ p = llr + (long long)blockIdx.x * n;
+  float s = 0.0f;
+  for (int v = threadIdx.x; v < n; v += blockDim.x) s += fabsf(__ldg(&p[v]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.0f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s_part[w];
+    key[blockIdx.x] = t;
+  }
+}
+
+// One CTA: bitonic sort of (key bits << 32 | frame) over the next power of two
+// (padding sorts last), ascending; non-negative keys order like their bits.
+__global__ void __launch_bounds__(1024) key_order_kernel(const float* __restrict__ key, int frames, int P,
+                                                         int64_t* __restrict__ order) {
+  extern __shared__ unsigned long long kv[];
+  const int tid = threadIdx.x, NT = blockDim.x;
+  for (int i = tid; i < P; i += NT)
+    kv[i] = i < frames ? ((unsigned long long)__float_as_uint(key[i]) << 32) | (unsigned)i : ~0ull;
+  __syncthreads();
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < P; i += NT) {
+        const int l = i ^ j;
+        if (l > i) {
+          const unsigned long long x = kv[i], y = kv[l];
+          if ((x > y) == ((i & k) == 0)) {
+            kv[i] = y;
+            kv[l] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = tid; i < frames; i += NT) order[i] = (int64_t)(kv[i] & 0xffffffffull);
+}
+
+cudaError_t launch_key_order(const float* llr, int n, int64_t frames, float* key, int64_t* order, cudaStream_t st) {
+  if (frames <= 0 || frames > kKeyOrderMax) return cudaErrorInvalidValue;
+  int P = 1;
+  while (P < frames) P <<= 1;
+  cudaError_t e = cudaFuncSetAttribute(key_order_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kKeyOrderMax * 8);
+  if (e != cudaSuccess) return e;
+  frame_key_kernel<<<(unsigned)frames, 256, 0, st>>>(llr, n, key);
+  key_order_kernel<<<1, 1024, (size_t)P * 8, st>>>(key, (int)frames, P, order);
+  return cudaGetLastError();
+}
+
 // Flooding-schedule kernel for (algorithm, message type, degree bucket).
 const void* flood_kernel_ptr(int algo, int msg16, int dcmax) {
   switch (algo) {

@@ -207,6 +207,10 @@ const void* flood_kernel_ptr(int algo, int msg16, int dcmax);
 // ascending rank, ids outside [0, ncodes) last; ascending frame index within a group.
 cudaError_t launch_mixed_order(const int32_t* code_id, int64_t frames, const int32_t* rank_of, int ncodes,
                                int64_t* order, cudaStream_t st);
+// Frame order of a single-code batch, hardest frames first: ascending sum of
+// |LLR| per frame (ties by frame index).  frames <= kKeyOrderMax; key: frames floats.
+constexpr int kKeyOrderMax = 16384;
+cudaError_t launch_key_order(const float* llr, int n, int64_t frames, float* key, int64_t* order, cudaStream_t st);
 int state_dcmax_bucket(int max_dc);
 int state_flood_threads();
 const void* state_flood_kernel_ptr(int dcmax, bool all_smem);
