@@ -169,7 +169,10 @@ int gf2c_decoder_destroy(gf2c_decoder* dec);
  *   converged   frames uint8: DecoderResult::converged             (nullable)
  *   syndrome_ok frames uint8: DecoderResult::syndrome_check_passed (nullable)
  *   beliefs     frames x n f32 final posterior LLRs                (nullable)
- * frames == 0 is a no-op. */
+ * frames == 0 is a no-op.  Each frame's results depend on that frame only; a batch
+ * of more frames than the decoder runs at once (up to 16384) is decoded hardest
+ * frames first (two small kernels order the frames by their sum of |LLR|), so
+ * the device-memory path launches 1 or 3 kernels (gf2c_decoder_last_launches). */
 int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32_t max_iter,
                       uint64_t* msg_bits, int32_t* iterations, uint8_t* converged,
                       uint8_t* syndrome_ok, float* beliefs, int32_t mem, void* stream);
