@@ -617,12 +617,13 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
   if (frames >= 2 * chunk && bl >= ((size_t)64 << 20) && pipeline_ready(dec)) {
     GF2C_CUDA(cudaEventRecord(dec->pev_fork, st));
     GF2C_CUDA(cudaStreamWaitEvent(dec->pstream, dec->pev_fork, 0));
-    // chunks: one wave of frames first (the copy that nothing overlaps is
-    // short), then the rest in three (fewer chunk boundaries)
+    // chunk sizes: one wave of frames first (the copy that nothing overlaps is
+    // short), then doubling, so that each copy is done before the SMs run out
+    // of decoding work; a remainder below the next size joins the last chunk
     int chunks = 0, launches = 0;
-    const int64_t big = std::max<int64_t>(dec->grid, (frames - dec->grid + 2) / 3);
-    for (int64_t f0 = 0, nf = 0; f0 < frames; f0 += nf, chunks++) {
-      nf = std::min(chunks == 0 ? (int64_t)dec->grid : big, frames - f0);
+    for (int64_t f0 = 0, nf = 0, want = dec->grid; f0 < frames; f0 += nf, chunks++, want *= 2) {
+      nf = std::min(want, frames - f0);
+      if (frames - f0 - nf < want) nf = frames - f0;
       const int slot = chunks & 1;
       cudaStream_t s = slot ? dec->pstream : st;
       const size_t ln = (size_t)nf * h.n * 4, lo = (size_t)f0 * h.n * 4;
