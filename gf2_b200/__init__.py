@@ -10,8 +10,8 @@ from .bch import BchCode, BchDecoder, BchEncoder
 from . import gf2io
 from .gf2io import DenseEncoder, EncodingCache
 from .ldpc import (AwgnChannel, BpskModulator, CirculantMatrix, CodeRate, DecoderResult, FrameSize, Llr,
-                   LdpcCode, LdpcDecoder, LdpcEncoder, QuasiCyclicLdpc, awgn_frames, pack_bits, sigma2_from_ebn0,
-                   unpack_bits, words)
+                   LdpcCode, LdpcDecoder, LdpcEncoder, QuasiCyclicLdpc, awgn_frames, judge_spa64, pack_bits,
+                   sigma2_from_ebn0, unpack_bits, words)
 
 ALGO_MINSUM = _capi.ALGO_MINSUM
 ALGO_SPA = _capi.ALGO_SPA
@@ -24,6 +24,6 @@ MSG_F16 = _capi.MSG_F16
 Gf2cError = _capi.Gf2cError
 
 __all__ = ["BchCode", "BchDecoder", "BchEncoder", "DenseEncoder", "EncodingCache", "gf2io", "AwgnChannel", "BpskModulator", "CirculantMatrix", "CodeRate", "DecoderResult", "FrameSize", "Llr",
-           "LdpcCode", "LdpcDecoder", "LdpcEncoder", "QuasiCyclicLdpc", "awgn_frames", "pack_bits",
+           "LdpcCode", "LdpcDecoder", "LdpcEncoder", "QuasiCyclicLdpc", "awgn_frames", "judge_spa64", "pack_bits",
            "sigma2_from_ebn0", "unpack_bits", "words", "ALGO_MINSUM", "ALGO_SPA", "ALGO_NMS", "ALGO_SPA_FAST", "SCHED_FLOODING",
            "SCHED_LAYERED", "MSG_F32", "MSG_F16", "Gf2cError"]

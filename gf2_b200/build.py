@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libgf2cuda.so")
-SOURCES = ["capi.cu", "code_host.cpp", "decode.cu", "layered.cu", "encode_channel.cu", "learned.cu", "noalloc.cu", "state_flood.cu", "bch.cu", "gf2io.cpp", "dense_encode.cu"]
+SOURCES = ["capi.cu", "code_host.cpp", "decode.cu", "layered.cu", "encode_channel.cu", "learned.cu", "noalloc.cu", "spa64.cu", "state_flood.cu", "bch.cu", "gf2io.cpp", "dense_encode.cu"]
 HEADERS = ["internal.h", "numeric.cuh", "dvbt2_tables.h", "../../include/gf2cuda.h"]
 
 

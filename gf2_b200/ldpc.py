@@ -607,5 +607,28 @@ def awgn_frames(code, seed, frame0, frames, sigma2, device=None, want_info=True,
     return info, cw, llr
 
 
+def judge_spa64(code, llr, max_iterations, schedule=C.SCHED_LAYERED, beliefs=False, stream=None):
+    """FP64 sum-product judge on the GPU (gf2c_judge_spa64): the precision
+    reference the FP32 / FP16 decoders are stated against.  llr: CUDA float32
+    tensor [F, n].  Returns a dict of device tensors like
+    LdpcDecoder.decode_tensors; beliefs are float64."""
+    import torch
+    if llr.dtype != torch.float32 or not llr.is_cuda or llr.dim() != 2 or llr.shape[1] != code.n():
+        raise ValueError("llr must be a CUDA float32 tensor [frames, n]")
+    llr = llr.contiguous()
+    F, dev = llr.shape[0], llr.device
+    out = dict(msg=torch.zeros((F, words(code.k())), dtype=torch.int64, device=dev),
+               iters=torch.zeros(F, dtype=torch.int32, device=dev),
+               conv=torch.zeros(F, dtype=torch.uint8, device=dev),
+               synd_ok=torch.zeros(F, dtype=torch.uint8, device=dev))
+    if beliefs:
+        out["beliefs"] = torch.zeros((F, code.n()), dtype=torch.float64, device=dev)
+    st = stream or torch.cuda.current_stream(dev)
+    C.check(C.lib.gf2c_judge_spa64(code.handle, int(schedule), _ptr(llr), F, int(max_iterations), _ptr(out["msg"]),
+                                   _ptr(out["iters"]), _ptr(out["conv"]), _ptr(out["synd_ok"]),
+                                   _ptr(out.get("beliefs")), _stream_ptr(st)))
+    return out
+
+
 def sigma2_from_ebn0(ebn0_db, rate):
     return C.lib.gf2c_sigma2_from_ebn0(float(ebn0_db), float(rate))

@@ -209,6 +209,20 @@ int gf2c_decode_batch_noalloc(const gf2c_code* code, const float* llr, int64_t f
                               uint64_t* msg_bits, int32_t* iterations, uint8_t* converged,
                               uint8_t* syndrome_ok, void* stream);
 
+/* FP64 sum-product judge -- no counterpart in the reference, whose sum-product
+ * (check_node_update_spa + Llr::boxplus_n, core.rs:762-787, llr.rs:210-215) is
+ * FP32 and unused.  The precision reference that the FP32 / FP16 decoders are
+ * stated against: 2 atanh(prod tanh(x/2)) with FP64 tanh / atanh, FP64
+ * messages and posteriors, |extrinsic product| <= 1 - 2^-50, flooding
+ * (core.rs:909-924) or layered schedule, syndrome early stop after every
+ * iteration.  Outputs as in gf2c_decode_batch except beliefs, which are FP64
+ * (frames x n, natural order).  Device memory only, asynchronous on `stream`;
+ * DVB-T2 and QC codes only (GF2C_ERR_UNSUPPORTED otherwise).  It keeps its own
+ * workspace per host thread (allocated on first use). */
+int gf2c_judge_spa64(const gf2c_code* code, int32_t schedule, const float* llr, int64_t frames, int32_t max_iter,
+                     uint64_t* msg_bits, int32_t* iterations, uint8_t* converged, uint8_t* syndrome_ok,
+                     double* beliefs, void* stream);
+
 /* Number of kernel launches issued by the last decode call of `dec`. */
 int gf2c_decoder_last_launches(const gf2c_decoder* dec, int32_t* launches);
 

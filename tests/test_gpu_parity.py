@@ -37,10 +37,10 @@ def assert_same_decode(gpu, ora, k, bitwise=True):
 
 
 def test_minsum_reference_parity_short_1_2(gpu, oracle):
-    """The BASELINE config-1 code and SNR: short 1/2, Eb/N0 1.0 dB, 50 iterations."""
+    """The full config-1 batch: short 1/2, 256 frames, Eb/N0 1.0 dB, 50 iterations."""
     code = g.LdpcCode.dvb_t2_short(g.CodeRate.Rate1_2)
     ocode = oracle.Code.dvbt2(1, 0)
-    _, _, llr = ocode.channel(1, 0, 64, 1.0)
+    _, _, llr = ocode.channel(1, 0, 256, 1.0)
     dec = g.LdpcDecoder(code)
     r = dec.decode_arrays(llr, 50, beliefs=True)
     assert_same_decode(r, ocode.decode(llr, 50), code.k(), bitwise=True)
@@ -87,9 +87,11 @@ def test_decoder_kats(gpu):
 
 @pytest.mark.parametrize("sched,msg16", [(0, False), (1, False), (1, True), (0, True)])
 def test_spa_parity(gpu, oracle, sched, msg16):
+    """Exact FP32 sum-product (flooding: the config-1 decoder) bit-exact against
+    its CPU restatement; the flooding FP32 case on the full 256-frame batch."""
     code = g.LdpcCode.dvb_t2_short(g.CodeRate.Rate1_2)
     ocode = oracle.Code.dvbt2(1, 0)
-    _, _, llr = ocode.channel(3, 0, 24, 1.0)
+    _, _, llr = ocode.channel(3, 0, 256 if (sched, msg16) == (0, False) else 24, 1.0)
     dec = g.LdpcDecoder(code, algorithm=g.ALGO_SPA, schedule=sched, msg_dtype=g.MSG_F16 if msg16 else g.MSG_F32)
     r = dec.decode_arrays(llr, 50, beliefs=True)
     assert_same_decode(r, ocode.decode(llr, 50, algo=1, sched=sched, msg16=msg16), code.k())
