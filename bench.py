@@ -165,18 +165,35 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def read_traffic(workload):
-    """DRAM bytes per launch from the committed ncu summary of the workload
-    (profiles/<kernel>_<workload>.md), if present."""
-    import glob
-    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", f"*_{workload}.md"))):
-        try:
-            for line in open(path):
-                if line.strip().startswith("traffic_bytes_per_launch:"):
-                    return float(line.split(":", 1)[1].split()[0])
-        except OSError:
-            pass
-    return None
+def source_hash(paths):
+    """sha256 over the named source files (paths relative to the repository)."""
+    import hashlib
+    h = hashlib.sha256()
+    for rel in paths:
+        with open(os.path.join(ROOT, rel), "rb") as f:
+            h.update(rel.encode() + b"\0" + f.read())
+    return h.hexdigest()
+
+
+def read_traffic(workload, frame_iters):
+    """DRAM bytes of the launch: the per-frame-iteration DRAM traffic of the
+    workload's dominant kernel from its ncu capture (profiles/traffic.json)
+    times the frame-iterations the timed launch executed.  None when there is
+    no capture or when the kernel's sources changed since it was taken (the
+    entry records the sha256 of the sources it profiled)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            e = json.load(f).get(workload)
+    except (OSError, ValueError):
+        return None, "no ncu capture"
+    if not e:
+        return None, "no ncu capture of this workload"
+    try:
+        if source_hash(e["sources"]) != e["source_sha256"]:
+            return None, "ncu capture predates the current kernel sources"
+    except OSError:
+        return None, "kernel sources missing"
+    return e["dram_bytes_per_frame_iteration"] * frame_iters, e["capture"]
 
 
 def measured_peak():
@@ -207,9 +224,20 @@ def run_cpu_reference(name, seed, steps, warmup, cores=None):
     frame, rate, max_iter, pts = cpu_reference_frames(name)
     code = pyoracle.Code.dvbt2(frame, rate)
     per = len(pts)
-    S = per * max(1, round(cores / per)) if per > 1 else max(1, cores)
-    eb = [pts[f % per] for f in range(S)]
-    _, _, llr = code.channel(seed, 0, S, eb)
+    # A multiple of the thread count, at least two frames per thread, grown
+    # until one pass takes about 10 s, so that no thread idles and the sample
+    # is a stable measure (frame f at Eb/N0 point f mod per).
+    S = cores * max(2, -(-per // cores))
+    for _ in range(6):
+        eb = [pts[f % per] for f in range(S)]
+        _, _, llr = code.channel(seed, 0, S, eb)
+        t0 = time.perf_counter()
+        code.decode_faithful(llr, max_iter, threads=cores)
+        dt = time.perf_counter() - t0
+        if dt >= 5.0:
+            break
+        S = cores * max(2 * (S // cores), int(-(-S * 10.0 / max(dt, 1e-3) // cores)))
+        S = min(S, cores * 256)
     times, iters = [], None
     for s in range(warmup + steps):
         t0 = time.perf_counter()
@@ -247,7 +275,7 @@ class SingleCode:
                                  msg_dtype=g.MSG_F16 if w["msg16"] else g.MSG_F32)
         self.out = None
         self.desc = w["desc"]
-        self.dtype = "f32"
+        self.dtype = "f16 storage / f32 math" if w["msg16"] else "f32"
         self.msg_bytes = 2 if w["msg16"] else 4
 
     def step(self):
@@ -264,7 +292,8 @@ class SingleCode:
         conv = self.out["conv"].cpu().numpy()
         c = self.code
         b = sum(alg_bytes(c.n(), c.k(), c.nnz(), self.msg_bytes, int(i)) for i in it)
-        return b, {"mean": float(it.mean()), "max": int(it.max()), "converged_frac": float(conv.mean())}
+        return b, {"mean": float(it.mean()), "max": int(it.max()), "converged_frac": float(conv.mean()),
+                   "frame_iterations": int(it.sum())}
 
     def host_step_factory(self):
         """The public C-ABI host path: pinned host LLRs in, results out."""
@@ -348,7 +377,7 @@ class Mixed:
                      f"sum-product (SFU) fp16, an ordering kernel (frames grouped by code) and one persistent decode launch "
                      f"from a CUDA graph, autotuned shape "
                      f"threads={threads} blocks/SM={bps or 'max'}")
-        self.dtype = "f32"
+        self.dtype = "f16 storage / f32 math"
 
     def step(self):
         self.dec.decode_mixed_tensors(self.llr, self.llr_off, self.cid, self.mit, self.msg, self.msg_off, self.iters,
@@ -368,7 +397,7 @@ class Mixed:
             code = self.codes[c]
             b += sum(alg_bytes(code.n(), code.k(), code.nnz(), 2, int(i)) for i in sel)
         return b, {"mean": float(it.mean()), "max": int(it.max()),
-                   "converged_frac": float(self.conv.float().mean().item())}
+                   "converged_frac": float(self.conv.float().mean().item()), "frame_iterations": int(it.sum())}
 
     def host_step_factory(self):
         import ctypes
@@ -800,6 +829,7 @@ def main():
     bits = wl.bits_per_step() * world
     value = bits * args.steps / (total_ms / 1e3) / 1e9
     bytes_launch, iters = wl.stats()
+    traffic, traffic_src = read_traffic(args.workload, iters.get("frame_iterations", 0))
     avg_launch_s = statistics.mean(step_ms) / 1e3
     achieved = bytes_launch / avg_launch_s / 1e9
     peak, peak_kind = measured_peak()
@@ -846,7 +876,7 @@ def main():
                 "config": config,
                 "iterations": iters,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": read_traffic(args.workload),
+                             "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
                              "peak_source": peak_kind, "algorithmic_bytes_per_launch": bytes_launch},
                 "gpu_launches": launches, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)

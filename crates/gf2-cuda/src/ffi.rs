@@ -115,6 +115,7 @@ extern "C" {
     pub fn gf2c_nms_trainer_create(code: *const gf2c_code, iterations: i32, max_frames: i64,
                                    out: *mut *mut gf2c_nms_trainer) -> i32;
     pub fn gf2c_nms_trainer_destroy(tr: *mut gf2c_nms_trainer) -> i32;
+    pub fn gf2c_nms_trainer_set_schedule(tr: *mut gf2c_nms_trainer, schedule: i32) -> i32;
     pub fn gf2c_nms_trainer_layers(tr: *const gf2c_nms_trainer, layers: *mut i32) -> i32;
     pub fn gf2c_nms_loss_grad(tr: *mut gf2c_nms_trainer, llr: *const f32, cw_bits: *const u64, frames: i64,
                               alpha: *const f32, beta: *const f32, grad_alpha: *mut f32, grad_beta: *mut f32,

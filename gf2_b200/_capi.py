@@ -36,7 +36,7 @@ EXPORTS = [
     "gf2c_decoder_create", "gf2c_decoder_create_multi", "gf2c_decoder_destroy",
     "gf2c_decode_batch", "gf2c_decode_mixed", "gf2c_decoder_last_launches", "gf2c_decode_batch_noalloc",
     "gf2c_judge_spa64",
-    "gf2c_nms_trainer_create", "gf2c_nms_trainer_destroy", "gf2c_nms_trainer_layers", "gf2c_nms_loss_grad",
+    "gf2c_nms_trainer_create", "gf2c_nms_trainer_destroy", "gf2c_nms_trainer_layers", "gf2c_nms_trainer_set_schedule", "gf2c_nms_loss_grad",
     "gf2c_adam_step", "gf2c_count_errors",
     "gf2c_bch_create_dvbt2", "gf2c_bch_destroy", "gf2c_bch_dims", "gf2c_bch_generator",
     "gf2c_bch_encode_batch", "gf2c_bch_decode_batch",
@@ -103,6 +103,7 @@ def _load():
     L.gf2c_nms_trainer_create.argtypes = [_vp, _i32, _i64, ctypes.POINTER(_vp)]
     L.gf2c_nms_trainer_destroy.argtypes = [_vp]
     L.gf2c_nms_trainer_layers.argtypes = [_vp, ctypes.POINTER(_i32)]
+    L.gf2c_nms_trainer_set_schedule.argtypes = [_vp, _i32]
     L.gf2c_nms_loss_grad.argtypes = [_vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.gf2c_count_errors.argtypes = [_vp, _vp, _i64, _i32, _vp, _vp, _vp]
     L.gf2c_adam_step.argtypes = [_vp, _vp, _vp, _vp, _i64, ctypes.c_float, ctypes.c_float, ctypes.c_float,

@@ -5,8 +5,9 @@ time; its launch shape is (threads per block, CTAs per SM), i.e. the check /
 variable tile a thread steps over and the number of frames in flight per SM.
 The autotuner times every feasible shape on a sample batch with CUDA events
 and keeps the fastest; results are cached in a JSON file keyed by device name,
-codes, algorithm, schedule and message type (GF2C_AUTOTUNE_CACHE overrides the
-default ~/.cache/gf2_b200/autotune.json).
+the build of the library (a hash of libgf2cuda.so), codes, algorithm, schedule
+and message type (GF2C_AUTOTUNE_CACHE overrides the default
+~/.cache/gf2_b200/autotune.json).
 """
 import json
 import os
@@ -36,9 +37,24 @@ def _store(d):
     os.replace(tmp, p)
 
 
+_LIB_HASH = None
+
+
+def library_hash():
+    """sha256 prefix of the loaded libgf2cuda.so: a shape timed on one build of
+    the kernels is not reused by another."""
+    global _LIB_HASH
+    if _LIB_HASH is None:
+        import hashlib
+        from . import _capi
+        with open(_capi.LIB_PATH, "rb") as f:
+            _LIB_HASH = hashlib.sha256(f.read()).hexdigest()[:16]
+    return _LIB_HASH
+
+
 def _key(codes, algorithm, schedule, msg_dtype, device_name):
     cs = ",".join(f"{c.n()}x{c.m()}x{c.nnz()}" for c in codes)
-    return f"{device_name}|{cs}|a{algorithm}|s{schedule}|m{msg_dtype}"
+    return f"{device_name}|lib {library_hash()}|{cs}|a{algorithm}|s{schedule}|m{msg_dtype}"
 
 
 def candidates(codes, schedule):

@@ -803,6 +803,7 @@ int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_of
 struct gf2c_nms_trainer {
   const gf2c_code* code = nullptr;
   int T = 0, L = 1;
+  int schedule = GF2C_SCHED_FLOODING;
   int64_t max_frames = 0;
   int grid = 0;
   long long work_stride = 0;
@@ -850,6 +851,16 @@ int gf2c_nms_trainer_layers(const gf2c_nms_trainer* tr, int32_t* layers) {
   return GF2C_OK;
 }
 
+int gf2c_nms_trainer_set_schedule(gf2c_nms_trainer* tr, int32_t schedule) {
+  if (!tr || (schedule != GF2C_SCHED_FLOODING && schedule != GF2C_SCHED_LAYERED))
+    return set_error(GF2C_ERR_INVALID_ARG, "bad arguments");
+  const HostCode& h = *tr->code->h;
+  if (schedule == GF2C_SCHED_LAYERED && (!h.layered_ok || h.max_nchk > 1024))
+    return set_error(GF2C_ERR_UNSUPPORTED, "layered training needs a QC or DVB-T2 code with Z <= 1024");
+  tr->schedule = schedule;
+  return GF2C_OK;
+}
+
 int gf2c_nms_loss_grad(gf2c_nms_trainer* tr, const float* llr, const uint64_t* cw_bits, int64_t frames,
                        const float* alpha, const float* beta, float* grad_alpha, float* grad_beta, float* loss,
                        float* soft_out, void* stream) {
@@ -860,6 +871,10 @@ int gf2c_nms_loss_grad(gf2c_nms_trainer* tr, const float* llr, const uint64_t* c
   const DevCode& h = tr->code->h->dev;
   const int grid = (int)std::min<int64_t>(tr->grid, frames);
   float* B = soft_out ? soft_out : (float*)tr->B.p;
+  if (tr->schedule == GF2C_SCHED_LAYERED)
+    return launch_nms_layered((const DevCode*)tr->dcode.p, h, tr->T, tr->L, llr, cw_bits, frames, alpha, beta,
+                              (float*)tr->X.p, B, (char*)tr->work.p, tr->work_stride, grid, (float*)tr->pf.p,
+                              grad_alpha, grad_beta, loss, st);
   int rc = launch_nms_forward((const DevCode*)tr->dcode.p, h, tr->T, tr->L, llr, cw_bits, frames, alpha, beta,
                               (float*)tr->X.p, B, (char*)tr->work.p, tr->work_stride, grid, (float*)tr->pf.p, st);
   if (rc) return rc;

@@ -227,6 +227,10 @@ int launch_nms_backward(const DevCode* dcode, const DevCode& h, int T, int L, co
                         long long frames, const float* alpha, const float* beta, const float* X, const float* B,
                         char* work, long long work_stride, int grid, float* pf, float* ga, float* gb,
                         float* loss, cudaStream_t st);
+int launch_nms_layered(const DevCode* dcode, const DevCode& h, int T, int L, const float* llr, const uint64_t* cw,
+                       long long frames, const float* alpha, const float* beta, float* X, float* B, char* work,
+                       long long work_stride, int grid, float* pf, float* ga, float* gb, float* loss,
+                       cudaStream_t st);
 int launch_count_errors(const uint64_t* a, const uint64_t* b, long long frames, int words, int32_t* per_frame,
                         unsigned long long* totals, cudaStream_t st);
 int launch_adam(float* p, const float* g, float* m1, float* m2, int count, float lr, float b1, float b2, float eps,

@@ -21,6 +21,8 @@
 // own row of a per-frame buffer, and nms_reduce_kernel sums the frames in
 // order.  Training is therefore bit-reproducible.
 // adam_kernel: Adam (Kingma & Ba 2015) with bias correction.
+#include <algorithm>
+
 #include "internal.h"
 #include "numeric.cuh"
 
@@ -253,6 +255,242 @@ __global__ void __launch_bounds__(kLearnThreads) nms_backward_kernel(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Layered schedule (no reference counterpart; the reference decoder floods).
+// Row groups g = 0 .. ncg-1 of iteration t, each check t' of g:
+//     x_e = A[v_e] - c_e,  c'_e = s_e * alpha[t,g] * max(m_e - beta[t,g], 0),
+//     A[v_e] += c'_e - c_e
+// with v2c formed from the posterior before the row group and the deltas of a
+// variable with several edges in one row group added in slot order (ascending
+// circulant shift) -- the arithmetic and the order of the layered inference
+// kernel (bp_layered_kernel, GF2C_ALGO_NMS, FP32 messages), so the training
+// forward and the inference decoder give the same posteriors bit for bit.
+// Backward, row groups in reverse order, with G = dL/dA after the row group and
+// P_e = dL/dc'_e from iteration t+1:
+//     dL/dc'_e = G[v_e] + P_e -> check-node backward (min routed to the first
+//     index attaining it) -> dL/dx_e;  P_e <- -G[v_e] - dL/dx_e;  G[v_e] += dL/dx_e
+// One CTA per frame, one thread per check of a row group (blockDim >= the
+// largest row group).  Weight gradients: per-check terms in shared memory,
+// summed per row group by warp 0 in a fixed order -- deterministic.
+// ---------------------------------------------------------------------------
+static constexpr int kLayThreadsMax = 1024;
+
+__global__ void __launch_bounds__(kLayThreadsMax) nms_layered_forward_kernel(
+    const DevCode* __restrict__ Cp, int T, int L, const float* __restrict__ llr, const uint64_t* __restrict__ cw,
+    long long frames, const float* __restrict__ alpha, const float* __restrict__ beta, float* __restrict__ X,
+    float* __restrict__ Bout, char* __restrict__ work, long long work_stride, float* __restrict__ pf) {
+  __shared__ float s_part[kLayThreadsMax / 32];
+  const DevCode& C = *Cp;
+  const int n = C.n, E = C.e_slots, ncg = C.ncg, tid = threadIdx.x;
+  const int* __restrict__ slot_var = C.slot_var;
+  float* c2v = (float*)(work + (long long)blockIdx.x * work_stride);
+  float* app = c2v + ((E + 63) & ~63);
+  const float scale = 1.0f / ((float)frames * (float)n);
+  for (long long f = blockIdx.x; f < frames; f += gridDim.x) {
+    const float* lf = llr + f * (long long)n;
+    for (int v = tid; v < n; v += blockDim.x) app[v] = lf[v];
+    __syncthreads();
+    for (int t = 0; t < T; t++) {
+      float* Xt = X + (f * T + t) * (long long)E;
+      for (int g = 0; g < ncg; g++) {
+        const int4 G = C.cg[g];
+        const uint32_t sync = C.cg_sync[g];
+        const int nchk = G.y, d = G.z;
+        const bool act = tid < nchk;
+        const int lay = (L == ncg) ? g : 0;
+        const float al = __ldg(&alpha[t * L + lay]), be = __ldg(&beta[t * L + lay]);
+        int vv[kLearnDcMax];
+        float dl[kLearnDcMax];
+        if (act) {
+          float ap[kLearnDcMax], o[kLearnDcMax];
+          float m1 = __int_as_float(0x7f800000), m2 = m1;
+          int i1 = -1, nreal = 0;
+          uint32_t neg = 0, negall = 0;
+          for (int i = 0; i < d; i++) {
+            const int s = G.w + i * nchk + tid;
+            const int v = __ldg(&slot_var[s]);
+            vv[i] = v;
+            if (v < 0) continue;
+            ap[i] = app[v];
+            o[i] = (t == 0) ? 0.0f : c2v[s];
+            const float x = __fsub_rn(ap[i], o[i]);
+            Xt[s] = x;
+            const float ax = fabsf(x);
+            if (ax < m1) {
+              m2 = m1;
+              m1 = ax;
+              i1 = i;
+            } else if (ax < m2) {
+              m2 = ax;
+            }
+            const uint32_t ng = (x < 0.0f) ? 1u : 0u;
+            neg |= ng << i;
+            negall ^= ng;
+            nreal++;
+          }
+          float mag1 = (nreal == 1) ? 0.0f : m1, mag2 = (nreal == 1) ? 0.0f : m2;
+          const float d1 = __fsub_rn(mag1, be), d2 = __fsub_rn(mag2, be);
+          mag1 = __fmul_rn(al, d1 > 0.0f ? d1 : 0.0f);
+          mag2 = __fmul_rn(al, d2 > 0.0f ? d2 : 0.0f);
+          for (int i = 0; i < d; i++) {
+            if (vv[i] < 0) continue;
+            const int s = G.w + i * nchk + tid;
+            const float mag = (i == i1) ? mag2 : mag1;
+            const float out = (negall ^ ((neg >> i) & 1u)) ? -mag : mag;
+            c2v[s] = out;
+            dl[i] = __fsub_rn(out, o[i]);
+            if (sync == 0) app[vv[i]] = __fadd_rn(ap[i], dl[i]);
+          }
+        }
+        if (sync != 0) {
+          __syncthreads();  // every pre-row-group posterior read
+          for (int i = 0; i < d; i++) {
+            if (act && vv[i] >= 0) app[vv[i]] = __fadd_rn(app[vv[i]], dl[i]);
+            if ((sync >> i) & 1u) __syncthreads();  // the next slot may hold the same variable
+          }
+        }
+        __syncthreads();
+      }
+    }
+    float part = 0.0f;
+    const uint64_t* cf = cw + f * (long long)C.words_n;
+    for (int v = tid; v < n; v += blockDim.x) {
+      const float b = app[v];
+      Bout[f * (long long)n + v] = b;
+      const float sv = ((cf[v >> 6] >> (v & 63)) & 1ull) ? -1.0f : 1.0f;
+      const float z = -sv * b;
+      part += (z > 0.0f ? z + log1pf(expf(-z)) : log1pf(expf(z))) * scale;
+    }
+    part = warp_sum_fixed(part);
+    if ((tid & 31) == 0) s_part[tid >> 5] = part;
+    __syncthreads();
+    if (tid == 0) {
+      float sum = 0.0f;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) sum = __fadd_rn(sum, s_part[w]);
+      pf[f * (2LL * T * L + 1) + 2 * T * L] = sum;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kLayThreadsMax) nms_layered_backward_kernel(
+    const DevCode* __restrict__ Cp, int T, int L, const uint64_t* __restrict__ cw, long long frames,
+    const float* __restrict__ alpha, const float* __restrict__ beta, const float* __restrict__ X,
+    const float* __restrict__ Bin, char* __restrict__ work, long long work_stride, float* __restrict__ pf) {
+  __shared__ float s_ga[kLayThreadsMax], s_gb[kLayThreadsMax];
+  const DevCode& C = *Cp;
+  const int n = C.n, E = C.e_slots, ncg = C.ncg, tid = threadIdx.x;
+  const int* __restrict__ slot_var = C.slot_var;
+  float* Gv = (float*)(work + (long long)blockIdx.x * work_stride);  // dL/dA, natural order
+  float* P = Gv + ((n + 63) & ~63);                                  // dL/dc from iteration t+1
+  const float scale = 1.0f / ((float)frames * (float)n);
+  for (long long f = blockIdx.x; f < frames; f += gridDim.x) {
+    const uint64_t* cf = cw + f * (long long)C.words_n;
+    for (int v = tid; v < n; v += blockDim.x) {
+      const float b = Bin[f * (long long)n + v];
+      const float sv = ((cf[v >> 6] >> (v & 63)) & 1ull) ? -1.0f : 1.0f;
+      const float z = -sv * b;
+      Gv[v] = scale * (1.0f / (1.0f + expf(-z))) * (-sv);
+    }
+    for (int s = tid; s < E; s += blockDim.x) P[s] = 0.0f;
+    __syncthreads();
+    float* row = pf + f * (2LL * T * L + 1);
+    for (int t = T - 1; t >= 0; t--) {
+      const float* Xt = X + (f * T + t) * (long long)E;
+      for (int g = ncg - 1; g >= 0; g--) {
+        const int4 G = C.cg[g];
+        const uint32_t sync = C.cg_sync[g];
+        const int nchk = G.y, d = G.z;
+        const bool act = tid < nchk;
+        const int lay = (L == ncg) ? g : 0;
+        const float al = __ldg(&alpha[t * L + lay]), be = __ldg(&beta[t * L + lay]);
+        int vv[kLearnDcMax];
+        float dx[kLearnDcMax];
+        if (act) {
+          float x[kLearnDcMax], gc[kLearnDcMax];
+          float m1 = __int_as_float(0x7f800000), m2 = m1;
+          int i1 = -1, i2 = -1, nreal = 0;
+          uint32_t neg = 0;
+          for (int i = 0; i < d; i++) {
+            const int s = G.w + i * nchk + tid;
+            const int v = __ldg(&slot_var[s]);
+            vv[i] = v;
+            dx[i] = 0.0f;
+            if (v < 0) continue;
+            gc[i] = __fadd_rn(Gv[v], P[s]);
+            x[i] = Xt[s];
+            const float ax = fabsf(x[i]);
+            if (ax < m1) {
+              m2 = m1;
+              i2 = i1;
+              m1 = ax;
+              i1 = i;
+            } else if (ax < m2) {
+              m2 = ax;
+              i2 = i;
+            }
+            neg ^= (x[i] < 0.0f) ? 1u : 0u;
+            nreal++;
+          }
+          float gA = 0.0f, gB = 0.0f, g1 = 0.0f, g2 = 0.0f;
+          if (nreal > 1) {
+            for (int i = 0; i < d; i++) {
+              if (vv[i] < 0) continue;
+              const float sg = ((neg ^ ((x[i] < 0.0f) ? 1u : 0u)) ? -1.0f : 1.0f);
+              const float u = ((i == i1) ? m2 : m1) - be;
+              if (u > 0.0f) {
+                gA += gc[i] * sg * u;
+                gB -= gc[i] * sg * al;
+                const float gm = gc[i] * sg * al;
+                if (i == i1) g2 += gm;  // the min over the others is slot i2
+                else g1 += gm;          // the min over the others is slot i1
+              }
+            }
+            if (i1 >= 0) dx[i1] = g1 * (x[i1] < 0.0f ? -1.0f : 1.0f);
+            if (i2 >= 0) dx[i2] = g2 * (x[i2] < 0.0f ? -1.0f : 1.0f);
+          }
+          for (int i = 0; i < d; i++) {
+            if (vv[i] < 0) continue;
+            P[G.w + i * nchk + tid] = -Gv[vv[i]] - dx[i];  // dL/dc of iteration t-1
+          }
+          s_ga[tid] = gA;
+          s_gb[tid] = gB;
+        }
+        __syncthreads();  // every read of G after the row group done
+        if (sync == 0) {
+          if (act)
+            for (int i = 0; i < d; i++)
+              if (vv[i] >= 0 && dx[i] != 0.0f) Gv[vv[i]] = __fadd_rn(Gv[vv[i]], dx[i]);
+        } else {
+          for (int i = 0; i < d; i++) {
+            if (act && vv[i] >= 0 && dx[i] != 0.0f) Gv[vv[i]] = __fadd_rn(Gv[vv[i]], dx[i]);
+            if ((sync >> i) & 1u) __syncthreads();
+          }
+        }
+        if (tid < 32) {
+          float sa = 0.0f, sb = 0.0f;
+          for (int c = tid; c < nchk; c += 32) {
+            sa = __fadd_rn(sa, s_ga[c]);
+            sb = __fadd_rn(sb, s_gb[c]);
+          }
+          sa = warp_sum_fixed(sa);
+          sb = warp_sum_fixed(sb);
+          if (tid == 0) {
+            if (L == ncg) {
+              row[t * L + lay] = sa;
+              row[T * L + t * L + lay] = sb;
+            } else {  // one weight pair per iteration: row groups summed in descending order
+              row[t * L] = (g == ncg - 1) ? sa : __fadd_rn(row[t * L], sa);
+              row[T * L + t * L] = (g == ncg - 1) ? sb : __fadd_rn(row[T * L + t * L], sb);
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+}
+
 // out[i] = sum over frames f (ascending) of pf[f][i], i < 2 T L + 1; warp per i.
 __global__ void nms_reduce_kernel(const float* __restrict__ pf, long long frames, int TL,
                                   float* __restrict__ grad_alpha, float* __restrict__ grad_beta,
@@ -299,6 +537,26 @@ int launch_nms_backward(const DevCode* dcode, const DevCode& h, int T, int L, co
                         float* loss, cudaStream_t st) {
   nms_backward_kernel<<<grid, kLearnThreads, 0, st>>>(dcode, T, L, llr, cw, frames, alpha, beta, X, B, work,
                                                       work_stride, pf);
+  GF2C_CUDA(cudaGetLastError());
+  const int outs = 2 * T * L + 1, warps = 8;
+  nms_reduce_kernel<<<(outs + warps - 1) / warps, warps * 32, 0, st>>>(pf, frames, T * L, ga, gb, loss);
+  GF2C_CUDA(cudaGetLastError());
+  return GF2C_OK;
+}
+
+int launch_nms_layered(const DevCode* dcode, const DevCode& h, int T, int L, const float* llr, const uint64_t* cw,
+                       long long frames, const float* alpha, const float* beta, float* X, float* B, char* work,
+                       long long work_stride, int grid, float* pf, float* ga, float* gb, float* loss,
+                       cudaStream_t st) {
+  if (h.max_dc > kLearnDcMax) return set_error(GF2C_ERR_UNSUPPORTED, "learned decoder: check degree above 32");
+  if (!h.layered_ok || h.max_nchk > kLayThreadsMax)
+    return set_error(GF2C_ERR_UNSUPPORTED, "layered training needs row groups of at most 1024 checks");
+  const int threads = std::max(32, (h.max_nchk + 31) / 32 * 32);
+  nms_layered_forward_kernel<<<grid, threads, 0, st>>>(dcode, T, L, llr, cw, frames, alpha, beta, X, B, work,
+                                                        work_stride, pf);
+  GF2C_CUDA(cudaGetLastError());
+  nms_layered_backward_kernel<<<grid, threads, 0, st>>>(dcode, T, L, cw, frames, alpha, beta, X, B, work,
+                                                         work_stride, pf);
   GF2C_CUDA(cudaGetLastError());
   const int outs = 2 * T * L + 1, warps = 8;
   nms_reduce_kernel<<<(outs + warps - 1) / warps, warps * 32, 0, st>>>(pf, frames, T * L, ga, gb, loss);

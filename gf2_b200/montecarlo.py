@@ -6,8 +6,16 @@ when the decoder does not converge or fails the syndrome, :157) and its
 simulation module only runs uncoded BER (SimulationRunner,
 crates/gf2-coding/src/simulation.rs:140-193).  Here one point runs batches of
 seeded frames (channel kernel -> decoder -> error-count kernel) until a target
-number of frame errors or a frame budget is reached.  A frame error is a
-decoded message that differs from the transmitted one.
+number of frame errors or a frame budget is reached.  Two frame-error counts
+are kept:
+  frame_errors          the decoded message differs from the transmitted one
+                        (what a receiver sees: undetected errors included,
+                        unconverged frames that happen to be right excluded)
+  frame_errors_ref_rule the reference example's rule, a frame that did not
+                        converge or failed the syndrome check
+                        (!converged || !syndrome_check_passed,
+                        examples/ldpc_awgn.rs:156-158)
+plus undetected_errors (syndrome satisfied, message wrong).
 
 Multi-GPU: frames are sharded by index (rank r of w decodes global frame
 indices b*batch*w + r*batch + i of batch b), there is no exchange during
@@ -55,6 +63,7 @@ def simulate_point(decoder, code, ebn0_db, max_iter, batch=1024, max_frames=1 <<
     device = device or torch.device("cuda", torch.cuda.current_device())
     k = code.k()
     totals = torch.zeros(2, dtype=torch.int64, device=device)  # frame errors, bit errors
+    ref_rule = torch.zeros(2, dtype=torch.int64, device=device)  # !conv || !synd_ok, undetected
     hist = torch.zeros(max_iter + 1, dtype=torch.int64, device=device)
     frames = 0
     b = 0
@@ -72,16 +81,23 @@ def simulate_point(decoder, code, ebn0_db, max_iter, batch=1024, max_frames=1 <<
                                         batch, words(k), None, ctypes.c_void_p(totals.data_ptr()),
                                         ctypes.c_void_p(st.cuda_stream)))
         hist += torch.bincount(out["iters"].long().clamp(0, max_iter), minlength=max_iter + 1)
+        failed = (out["conv"] == 0) | (out["synd_ok"] == 0)
+        wrong = (out["msg"] != info).any(dim=1)
+        ref_rule[0] += failed.sum()
+        ref_rule[1] += (wrong & (out["synd_ok"] != 0)).sum()
         frames += batch
         b += 1
         fe = int(totals[0].item()) * world  # estimate across ranks without a collective
         if frames * world >= max_frames or fe >= min_frame_errors:
             break
-    counters = torch.cat([totals, torch.tensor([frames], dtype=torch.int64, device=device), hist])
+    counters = torch.cat([totals, torch.tensor([frames], dtype=torch.int64, device=device), ref_rule, hist])
     reduce_counters(counters)
     fe, be, nf = int(counters[0]), int(counters[1]), int(counters[2])
-    h = counters[3:].cpu().numpy()
+    fr, ud = int(counters[3]), int(counters[4])
+    h = counters[5:].cpu().numpy()
     lo, hi = wilson(fe, nf)
     return dict(ebn0_db=float(ebn0_db) if ebn0_of_frame is None else None, frames=nf, frame_errors=fe,
                 bit_errors=be, fer=fe / nf if nf else 0.0, ber=be / (nf * k) if nf else 0.0, fer_ci=(lo, hi),
+                frame_errors_ref_rule=fr, fer_ref_rule=fr / nf if nf else 0.0, fer_ref_rule_ci=wilson(fr, nf),
+                undetected_errors=ud,
                 mean_iters=float((h * np.arange(len(h))).sum() / max(1, h.sum())), iter_hist=h.tolist())

@@ -24,6 +24,9 @@ Reported per point and decoder:
                      1 (and 5) iterations (frames whose iteration counts agree)
   rel_it1            max |L - L_judge| / max(|L_judge|, 1) after 1 iteration
   hd_frames          fraction of frames whose decoded message equals the judge's
+  hd_decoded         the same over the frames the judge decodes (converges on);
+                     frames no decoder decodes oscillate chaotically, so their
+                     decisions are not a precision measure
   hd_bits            fraction of equal message bits
   fer, fer_ci        frames whose message differs from the transmitted bits,
                      with the Wilson 95 % interval
@@ -95,8 +98,12 @@ def precision_point(code, ebn0, frames, seed, point, max_iter=50, decoders=None,
         fe = _frame_errors(full["msg"], info)
         nfe = int(fe.sum().item())
         bits = torch.from_numpy(unpack_bits(full["msg"].cpu().numpy().view(np.uint64), k))
+        same = (full["msg"] == jfull["msg"]).all(dim=1)
+        jc = jfull["conv"] != 0
         out[name] = dict(dev_it1=d1, rel_it1=rel1, dev_it5=d5,
-                         hd_frames=float((full["msg"] == jfull["msg"]).all(dim=1).float().mean().item()),
+                         hd_frames=float(same.float().mean().item()),
+                         hd_decoded=float(same[jc].float().mean().item()) if bool(jc.any()) else None,
+                         judge_decoded=int(jc.sum().item()),
                          hd_bits=float((bits == jbits).float().mean().item()),
                          fer=nfe / frames, fer_ci=wilson(nfe, frames), frame_errors=nfe,
                          fer_ref_rule=float((full["conv"] == 0).float().mean().item()),
@@ -120,8 +127,9 @@ def format_row(eb, r):
     parts = [f"{eb:.1f} dB judge FER {r['judge_fp64']['fer']:.4f}"]
     for name, _, _ in DECODERS:
         x = r[name]
+        hd = "-" if x["hd_decoded"] is None else f"{x['hd_decoded']:.4f}"
         parts.append(f"{name}: dev1 {x['dev_it1']:.2e} dev5 {x['dev_it5']:.2e} hd {x['hd_frames']:.4f} "
-                     f"FER {x['fer']:.4f}")
+                     f"hd(decoded) {hd} FER {x['fer']:.4f}")
     return " | ".join(parts)
 
 

@@ -237,7 +237,13 @@ int gf2c_nms_trainer_create(const gf2c_code* code, int32_t iterations, int64_t m
                             gf2c_nms_trainer** out);
 int gf2c_nms_trainer_destroy(gf2c_nms_trainer* tr);
 int gf2c_nms_trainer_layers(const gf2c_nms_trainer* tr, int32_t* layers);
-/* Forward (iterations flooding steps, no early stop) and backward over a device
+/* Schedule of the unrolled decoder the trainer differentiates: GF2C_SCHED_FLOODING
+ * (the default, decode_iterative's schedule) or GF2C_SCHED_LAYERED (row groups
+ * in order, the posterior updated after each; weights per iteration and row
+ * group; the forward equals the layered GF2C_ALGO_NMS decoder with FP32
+ * messages bit for bit).  GF2C_ERR_UNSUPPORTED for codes without row groups. */
+int gf2c_nms_trainer_set_schedule(gf2c_nms_trainer* tr, int32_t schedule);
+/* Forward (iterations steps of the trainer's schedule, no early stop) and backward over a device
  * batch: llr [frames][n] f32, cw_bits [frames][ceil(n/64)] transmitted codewords,
  * alpha / beta [iterations][layers].  Writes the mean binary cross-entropy of
  * sigmoid(final LLR) against the codeword bits to *loss and its gradients to

@@ -109,6 +109,13 @@ double or_nms_loss_grad(const or_code* c, const float* llr, const uint8_t* cw,
                         int64_t frames, int T, const double* alpha, const double* beta,
                         double* grad_alpha, double* grad_beta, double* out_llr);
 
+/* The same with the layered schedule (row groups in order, posterior updated
+ * after each row group, weights per iteration and row group); NaN and an error
+ * message for codes without row groups. */
+double or_nms_layered_loss_grad(const or_code* c, const float* llr, const uint8_t* cw,
+                                int64_t frames, int T, const double* alpha, const double* beta,
+                                double* grad_alpha, double* grad_beta, double* out_llr);
+
 /* IEEE binary16 round-to-nearest-even conversion, for message storage */
 uint16_t or_f32_to_f16(float x);
 float or_f16_to_f32(uint16_t h);

@@ -66,6 +66,9 @@ def lib():
         L.or_own_sincos2pi.argtypes = [ctypes.c_double, _f64p, _f64p]
         L.or_shannon_limit.restype = ctypes.c_double
         L.or_shannon_limit.argtypes = [ctypes.c_double]
+        L.or_nms_layered_loss_grad.restype = ctypes.c_double
+        L.or_nms_layered_loss_grad.argtypes = [ctypes.c_void_p, _f32p, _u8p, ctypes.c_int64, ctypes.c_int,
+                                               _f64p, _f64p, _f64p, _f64p, _f64p]
         L.or_nms_loss_grad.restype = ctypes.c_double
         L.or_nms_loss_grad.argtypes = [ctypes.c_void_p, _f32p, _u8p, ctypes.c_int64, ctypes.c_int,
                                        _f64p, _f64p, _f64p, _f64p, _f64p]
@@ -228,7 +231,7 @@ class Code:
             raise OracleError(lib().or_last_error().decode())
         return info, cw, llr
 
-    def nms_loss_grad(self, llr, cw, T, alpha, beta):
+    def nms_loss_grad(self, llr, cw, T, alpha, beta, layered=False):
         llr = np.ascontiguousarray(llr, np.float32).reshape(-1, self.n)
         cw = np.ascontiguousarray(cw, np.uint8).reshape(-1, self.n)
         a = np.ascontiguousarray(alpha, np.float64)
@@ -236,9 +239,11 @@ class Code:
         ga = np.zeros_like(a)
         gb = np.zeros_like(b)
         out = np.zeros(llr.shape, np.float64)
-        loss = lib().or_nms_loss_grad(self.h, _p(llr, _f32p), _p(cw, _u8p), llr.shape[0], T,
-                                      _p(a, _f64p), _p(b, _f64p), _p(ga, _f64p), _p(gb, _f64p),
-                                      _p(out, _f64p))
+        fn = lib().or_nms_layered_loss_grad if layered else lib().or_nms_loss_grad
+        loss = fn(self.h, _p(llr, _f32p), _p(cw, _u8p), llr.shape[0], T,
+                  _p(a, _f64p), _p(b, _f64p), _p(ga, _f64p), _p(gb, _f64p), _p(out, _f64p))
+        if loss != loss:
+            raise OracleError(lib().or_last_error().decode())
         return loss, ga, gb, out
 
 

@@ -9,7 +9,9 @@ Config 2 (normal 3/5, layered, FP16 / FP32 message storage, exact and SFU
 sum-product): one Eb/N0 point of the 0.6..1.4 dB sweep at 1024 frames through
 gf2_b200.precision (the full sweep is `python -m gf2_b200.precision`):
 decisions equal to the judge's on the frames it decodes, FER within the
-judge's Wilson interval, bounded one- and five-iteration deviations.
+judge's Wilson interval, bounded one- and five-iteration deviations.  A frame
+that no decoder decodes oscillates chaotically, so decision agreement is
+measured on the frames the judge decodes.
 """
 import numpy as np
 import pytest
@@ -51,10 +53,11 @@ def test_config2_precision_point(gpu):
     for name, _, _ in precision.DECODERS:
         x = r[name]
         assert x["hd_bits"] > 0.999, (name, x)
-        assert x["hd_frames"] > 0.9, (name, x)
-        assert lo - 0.03 <= x["fer"] <= hi + 0.03, (name, x, jf)
-        assert np.isfinite(x["dev_it1"]) and np.isfinite(x["dev_it5"])
-    assert r["spa_exact_f32"]["dev_it1"] < 0.05, r["spa_exact_f32"]
-    assert r["spa_exact_f16"]["dev_it1"] < 0.2, r["spa_exact_f16"]
-    assert r["spa_fast_f32"]["dev_it1"] < 0.2, r["spa_fast_f32"]
-    assert r["spa_fast_f16"]["dev_it1"] < 0.3, r["spa_fast_f16"]
+        assert x["judge_decoded"] > 500 and x["hd_decoded"] >= 0.995, (name, x)
+        assert lo <= x["fer"] <= hi, (name, x, jf)
+    # one- and five-iteration posterior deviations (measured on this point:
+    # FP32 storage ~2e-5 / 1.5e-4, FP16 storage ~3e-3 / 9e-3)
+    for name in ("spa_exact_f32", "spa_fast_f32"):
+        assert r[name]["dev_it1"] < 2e-4 and r[name]["dev_it5"] < 2e-3, r[name]
+    for name in ("spa_exact_f16", "spa_fast_f16"):
+        assert r[name]["dev_it1"] < 1e-2 and r[name]["dev_it5"] < 5e-2, r[name]

@@ -260,3 +260,41 @@ def test_nms_gradient_fd(oracle):
             lm = c.nms_loss_grad(llr, cw, T, m if arr is a else a, m if arr is b else b)[0]
             fd = (lp - lm) / (2 * h)
             assert abs(fd - g[idx]) <= 1e-6 + 1e-4 * abs(fd)
+
+
+@pytest.mark.parametrize("frame,rate", [(1, 5), (1, 0), (0, 5)])
+def test_nms_layered_gradient_fd(oracle, frame, rate):
+    """FP64 layered learned-min-sum gradient against central finite differences;
+    normal 5/6 has row groups with up to 4 circulants in one block (repeated
+    variables inside a layer)."""
+    c = oracle.Code.dvbt2(frame, rate)
+    info, cw, llr = c.channel(9, 0, 1 if frame == 0 else 2, 3.0 if rate == 5 else 1.4)
+    T, L = 3, c.layers
+    rng = np.random.default_rng(2)
+    a = 0.8 + 0.1 * rng.random(T * L)
+    b = 0.1 + 0.1 * rng.random(T * L)
+    loss, ga, gb, out = c.nms_loss_grad(llr, cw, T, a, b, layered=True)
+    assert np.isfinite(loss) and np.abs(ga).max() > 0
+    for idx in (0, L + 3, 2 * L + 5, T * L - 1):
+        for arr, g in ((a, ga), (b, gb)):
+            h = 1e-6
+            p = arr.copy(); p[idx] += h
+            m = arr.copy(); m[idx] -= h
+            lp = c.nms_loss_grad(llr, cw, T, p if arr is a else a, p if arr is b else b, layered=True)[0]
+            lm = c.nms_loss_grad(llr, cw, T, m if arr is a else a, m if arr is b else b, layered=True)[0]
+            fd = (lp - lm) / (2 * h)
+            assert abs(fd - g[idx]) <= 1e-6 + 1e-4 * abs(fd), (idx, fd, g[idx])
+
+
+def test_nms_layered_forward_equals_layered_decoder(oracle):
+    """With alpha = 1, beta = 0 the layered training forward is plain layered
+    min-sum: its final posterior equals the layered min-sum oracle decoder's
+    (FP64 vs FP32 values, same decisions)."""
+    c = oracle.Code.dvbt2(1, 0)
+    info, cw, llr = c.channel(3, 0, 3, 1.6)
+    T, L = 4, c.layers
+    _, _, _, out = c.nms_loss_grad(llr, cw, T, np.ones(T * L), np.zeros(T * L), layered=True)
+    r = c.decode(llr, T, algo=3, sched=1, alpha=np.ones((T, L), np.float32), beta=np.zeros((T, L), np.float32))
+    ran = r["iters"] == T
+    assert ran.any()
+    assert np.allclose(out[ran], r["beliefs"][ran], rtol=1e-4, atol=1e-4)
