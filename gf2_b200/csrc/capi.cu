@@ -377,8 +377,8 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   for (auto* c : d->codes)
     if (smem_of((int)c->h->n) <= (size_t)kSmemBudget) d->smem_app_floats = std::max(d->smem_app_floats, (int)c->h->n);
   d->smem = smem_of(d->smem_app_floats);
-  if (layered && o.algorithm == GF2C_ALGO_SPA_FAST) {
-    // row groups with repeated variables: old messages / deltas of every slot
+  if (layered && o.algorithm != GF2C_ALGO_SPA) {
+    // row groups with repeated variables: deltas of every slot (fused row paths)
     int fl = 0;
     for (auto* c : d->codes)
       for (size_t g = 0; g < c->h->cg.size(); g++)

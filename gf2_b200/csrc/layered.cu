@@ -250,6 +250,126 @@ __device__ __forceinline__ void spa_fast_rep_b(const int2* __restrict__ sd, int 
   }
 }
 
+// Min-sum / normalised-offset min-sum update of check t of a row group whose D
+// slots all hold an edge and whose variables are all distinct: loads, check
+// node, message stores and posterior updates in one pass, with the arithmetic
+// of the general path of layered_iterations (v2c = APP - c2v_old, min1 / min2
+// / first argmin, sign parity, sign * alpha * max(min - beta, 0), the stored
+// message rounded through the message type, APP + (c2v_new - c2v_old)), so
+// results are bit-identical.  PART: the row group has d < D slots; slots
+// d..D-1 are absent (no load, no store).
+template <int ALGO, int MSG16, int D, bool PART>
+__device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
+                                       typename MsgIO<MSG16>::T* __restrict__ c2v, bool first, float al, float be,
+                                       const LayerSmem& S, const int2* __restrict__ vg, const int* __restrict__ ci,
+                                       int vgs, int d) {
+  typedef MsgIO<MSG16> IO;
+  float ap[D], o[D];
+#pragma unroll
+  for (int i = 0; i < D; i++) ap[i] = (!PART || i < d) ? app[slot_u(__ldg(&sd[i]), t, nchk)] : 0.0f;
+#pragma unroll
+  for (int i = 0; i < D; i++) o[i] = (first || (PART && i >= d)) ? 0.0f : ld_msg<MSG16>(c2v, s0 + i * nchk);
+  float m1 = __int_as_float(0x7f800000), m2 = m1;
+  int i1 = -1;
+  uint32_t neg = 0, apneg = 0;
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    if (PART && i >= d) continue;
+    const float w = __fsub_rn(ap[i], o[i]);
+    const float ax = fabsf(w);
+    if (ax < m1) {
+      m2 = m1;
+      m1 = ax;
+      i1 = i;
+    } else if (ax < m2) {
+      m2 = ax;
+    }
+    neg |= (uint32_t)(w < 0.0f) << i;
+    apneg |= (uint32_t)(ap[i] < 0.0f) << i;
+  }
+  float mag1 = m1, mag2 = m2;  // d >= 2 edges: never a single-edge check
+  if (ALGO == L_NMS) {
+    const float d1 = __fsub_rn(mag1, be), d2 = __fsub_rn(mag2, be);
+    mag1 = __fmul_rn(al, d1 > 0.0f ? d1 : 0.0f);
+    mag2 = __fmul_rn(al, d2 > 0.0f ? d2 : 0.0f);
+  }
+  const uint32_t negp = __popc(neg) & 1u;
+  uint32_t flips = 0;
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    if (PART && i >= d) continue;
+    const float mag = (i == i1) ? mag2 : mag1;
+    const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
+    st_msg<MSG16>(c2v, s0 + i * nchk, out);
+    const float nw = __fadd_rn(ap[i], __fsub_rn(out, o[i]));
+    app[slot_u(__ldg(&sd[i]), t, nchk)] = nw;
+    flips |= (uint32_t)(((apneg >> i) & 1u) != (uint32_t)(nw < 0.0f)) << i;
+  }
+  while (flips) {  // rare after the first iterations
+    const int i = __ffs(flips) - 1;
+    flips &= flips - 1;
+    flip_var(slot_u(__ldg(&sd[i]), t, nchk), S, vg, ci, vgs);
+  }
+}
+
+// Phase A of a min-sum / normalised-offset min-sum row group with repeated
+// variables (the counterpart of spa_fast_rep_a): the same check node as
+// ms_row; slots inside a run of one block leave their delta in dbuf for phase
+// B (spa_fast_rep_b, after one barrier), the other slots update their unique
+// variable now.  Same additions in the same order as the slot-by-slot general
+// path, so results are bit-identical.
+template <int ALGO, int MSG16, int D, bool PART>
+__device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
+                                         typename MsgIO<MSG16>::T* __restrict__ c2v, bool first, float al, float be,
+                                         uint32_t sync, float* dbuf, const LayerSmem& S,
+                                         const int2* __restrict__ vg, const int* __restrict__ ci, int vgs, int d) {
+  typedef MsgIO<MSG16> IO;
+  const uint32_t rep = sync | (sync << 1);  // slots inside a run
+  float ap[D], o[D];
+#pragma unroll
+  for (int i = 0; i < D; i++) ap[i] = (!PART || i < d) ? app[slot_u(__ldg(&sd[i]), t, nchk)] : 0.0f;
+#pragma unroll
+  for (int i = 0; i < D; i++) o[i] = (first || (PART && i >= d)) ? 0.0f : ld_msg<MSG16>(c2v, s0 + i * nchk);
+  float m1 = __int_as_float(0x7f800000), m2 = m1;
+  int i1 = -1;
+  uint32_t neg = 0;
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    if (PART && i >= d) continue;
+    const float w = __fsub_rn(ap[i], o[i]);
+    const float ax = fabsf(w);
+    if (ax < m1) {
+      m2 = m1;
+      m1 = ax;
+      i1 = i;
+    } else if (ax < m2) {
+      m2 = ax;
+    }
+    neg |= (uint32_t)(w < 0.0f) << i;
+  }
+  float mag1 = m1, mag2 = m2;
+  if (ALGO == L_NMS) {
+    const float d1 = __fsub_rn(mag1, be), d2 = __fsub_rn(mag2, be);
+    mag1 = __fmul_rn(al, d1 > 0.0f ? d1 : 0.0f);
+    mag2 = __fmul_rn(al, d2 > 0.0f ? d2 : 0.0f);
+  }
+  const uint32_t negp = __popc(neg) & 1u;
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    if (PART && i >= d) continue;
+    const float mag = (i == i1) ? mag2 : mag1;
+    const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
+    st_msg<MSG16>(c2v, s0 + i * nchk, out);
+    const float delta = __fsub_rn(out, o[i]);
+    if ((rep >> i) & 1u) {
+      dbuf[i * nchk + t] = delta;
+    } else {
+      const int v = slot_u(__ldg(&sd[i]), t, nchk);
+      app_put(app, v, ap[i] < 0.0f, __fadd_rn(ap[i], delta), S, vg, ci, vgs);
+    }
+  }
+}
+
 // Iterations of one frame with row groups of at most DCMAX slots; returns the
 // iteration count and whether the syndrome test passed at an early stop.
 template <int ALGO, int MSG16, int DCMAX>
@@ -267,6 +387,8 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
   const int* __restrict__ vg_chk = C.sp_ci;
   it = 0;
   converged = 0;
+  // fused row paths: every algorithm but the exact sum-product
+  constexpr bool kFused = (ALGO == L_SPA_FAST || ALGO == L_MS || ALGO == L_NMS) && DCMAX <= 22;
   for (;;) {
     const int tw = (a.nms_iters > 0) ? min(it, a.nms_iters - 1) : 0;
     const bool first = (it == 0);
@@ -284,22 +406,46 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
       const uint32_t ab = (act && t == 0) ? __ldg(&absent[g]) : 0u;
       // row group with repeated variables, all slots real everywhere: one barrier
       // (fewer slots than DCMAX: the PART variants)
-      const bool rep_row = ALGO == L_SPA_FAST && DCMAX <= 22 && S.dbuf != nullptr && sync != 0 && d >= 2 &&
-                           d <= DCMAX && __ldg(&absent[g]) == 0u;
+      const bool rep_row = kFused && S.dbuf != nullptr && sync != 0 && d >= 2 && d <= DCMAX &&
+                           __ldg(&absent[g]) == 0u;
+      float al = 1.0f, be = 0.0f;
+      if (ALGO == L_NMS) {
+        const int lay = (a.nms_L == ncg) ? g : 0;
+        al = __ldg(&a.alpha[tw * a.nms_L + lay]);
+        be = __ldg(&a.beta[tw * a.nms_L + lay]);
+      }
       if (rep_row) {
         if (act) {
-          if (d == DCMAX)
-            spa_fast_rep_a<MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, first, sync, S.dbuf, S, vg, vg_chk, vgs, d);
-          else
-            spa_fast_rep_a<MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, first, sync, S.dbuf, S, vg, vg_chk, vgs, d);
+          if constexpr (ALGO == L_SPA_FAST) {
+            if (d == DCMAX)
+              spa_fast_rep_a<MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, first, sync, S.dbuf, S, vg, vg_chk, vgs,
+                                                  d);
+            else
+              spa_fast_rep_a<MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, first, sync, S.dbuf, S, vg, vg_chk, vgs,
+                                                 d);
+          } else if constexpr (kFused) {
+            if (d == DCMAX)
+              ms_rep_a<ALGO, MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, first, al, be, sync, S.dbuf, S, vg,
+                                                  vg_chk, vgs, d);
+            else
+              ms_rep_a<ALGO, MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, first, al, be, sync, S.dbuf, S, vg,
+                                                 vg_chk, vgs, d);
+          }
         }
         __syncthreads();
         if (act) spa_fast_rep_b<DCMAX>(sd, t, nchk, app, sync, S.dbuf, S, vg, vg_chk, vgs);
-      } else if (ALGO == L_SPA_FAST && DCMAX <= 22 && act && sync == 0 && d >= 2 && d <= DCMAX && ab == 0) {
-        if (d == DCMAX)
-          spa_fast_row<MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs, d);
-        else
-          spa_fast_row<MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs, d);
+      } else if (kFused && act && sync == 0 && d >= 2 && d <= DCMAX && ab == 0) {
+        if constexpr (ALGO == L_SPA_FAST) {
+          if (d == DCMAX)
+            spa_fast_row<MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs, d);
+          else
+            spa_fast_row<MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs, d);
+        } else if constexpr (kFused) {
+          if (d == DCMAX)
+            ms_row<ALGO, MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, first, al, be, S, vg, vg_chk, vgs, d);
+          else
+            ms_row<ALGO, MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, first, al, be, S, vg, vg_chk, vgs, d);
+        }
       } else if (act) {
         // 1. indices, 2. all loads, 3. arithmetic
 #pragma unroll
@@ -340,9 +486,6 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
           }
           float mag1 = single ? 0.0f : m1, mag2 = single ? 0.0f : m2;
           if (ALGO == L_NMS) {
-            const int lay = (a.nms_L == ncg) ? g : 0;
-            const float al = __ldg(&a.alpha[tw * a.nms_L + lay]);
-            const float be = __ldg(&a.beta[tw * a.nms_L + lay]);
             const float d1 = __fsub_rn(mag1, be), d2 = __fsub_rn(mag2, be);
             mag1 = __fmul_rn(al, d1 > 0.0f ? d1 : 0.0f);
             mag2 = __fmul_rn(al, d2 > 0.0f ? d2 : 0.0f);
