@@ -62,6 +62,7 @@ struct gf2c_decoder {
   int max_n = 0, max_m = 0, max_words_k = 0, max_e_slots = 0, max_dc = 0, max_nchk = 0;
   int dcmax = 0, threads = 0, grid = 0, bitmap_words = 0, parity_words = 0, smem_app_floats = 0;
   int lay_dbuf_off = 0, lay_dbuf_floats = 0;
+  int lay_stage_off = 0, lay_stage_bytes = 0;
   const void* kernel = nullptr;
   bool state_flood = false;  // check-state flooding min-sum kernel (state_flood.cu)
   int sf_app_soff = 0;
@@ -457,6 +458,37 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
       d->lay_dbuf_floats = 0;
     }
   }
+  // Layered decoding of one code with a fused-row algorithm: the old messages
+  // of each row group are staged in shared memory by TMA bulk copies (a row
+  // group's messages are one contiguous block, which must start and end on a
+  // 16-byte boundary; three or more row groups), where this costs no occupancy.
+  if (layered && d->codes.size() == 1 && o.algorithm != GF2C_ALGO_SPA && threads <= 384 &&
+      !std::getenv("GF2C_NO_STAGE")) {
+    const HostCode& h = *d->codes[0]->h;
+    bool ok = h.cg.size() >= 3;
+    size_t mx = 0;
+    for (const int4& G : h.cg) {
+      const size_t off = (size_t)G.w * msg_bytes, by = (size_t)G.z * G.y * msg_bytes;
+      ok = ok && off % 16 == 0 && by % 16 == 0;
+      mx = std::max(mx, by);
+    }
+    const void* k = ok ? layered_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax, threads, true) : nullptr;
+    int optin = 0, occ0 = 0, occ1 = 0;
+    GF2C_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->dev));
+    const size_t off = (d->smem + 15) & ~(size_t)15, with = off + 2 * mx + 16;
+    if (k && with <= (size_t)optin) {
+      GF2C_CUDA(cudaFuncSetAttribute(d->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d->smem));
+      GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, d->kernel, threads, d->smem));
+      GF2C_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)with));
+      GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, k, threads, with));
+      if (occ1 > 0 && (occ1 >= occ0 || std::getenv("GF2C_FORCE_STAGE"))) {
+        d->kernel = k;
+        d->smem = with;
+        d->lay_stage_off = (int)off;
+        d->lay_stage_bytes = (int)mx;
+      }
+    }
+  }
   GF2C_CUDA(cudaFuncSetAttribute(d->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d->smem));
   int occ = 0;
   GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, d->kernel, threads, d->smem));
@@ -500,6 +532,8 @@ static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaSt
   a.parity_words = d->parity_words;
   a.lay_dbuf_off = d->lay_dbuf_off;
   a.lay_dbuf_floats = d->lay_dbuf_floats;
+  a.lay_stage_off = d->lay_stage_off;
+  a.lay_stage_bytes = d->lay_stage_bytes;
   a.alpha = (const float*)d->alpha.p;
   a.beta = (const float*)d->beta.p;
   a.nms_iters = d->opts.algorithm == GF2C_ALGO_NMS ? d->nms_iters : 0;
@@ -551,6 +585,7 @@ static int check_status(gf2c_decoder* d, cudaStream_t st) {
   GF2C_CUDA(cudaStreamSynchronize(st));
   if (h) {
     cudaMemsetAsync(d->status.p, 0, sizeof(int), st);
+    if (h == 2) return set_error(GF2C_ERR_KERNEL, "a staged message copy did not complete in time");
     return set_error(GF2C_ERR_INVALID_ARG, "a frame referenced a code id outside the decoder's codes");
   }
   return GF2C_OK;

@@ -187,7 +187,9 @@ struct DecodeArgs {
   int smem_app_floats;             // APP kept in shared memory when n <= this
   int bitmap_words;                // 32-bit words of the hard-decision bitmap
   int parity_words;                // 32-bit words of the check-parity bitmap (layered)
-  int lay_dbuf_off, lay_dbuf_floats;  // layered SPA_FAST: shared-memory buffer of slots x checks
+  int lay_dbuf_off, lay_dbuf_floats;  // layered fused rows: shared-memory buffer of slots x checks
+  int lay_stage_off, lay_stage_bytes; // layered, TMA-staged messages: two buffers of one row group's
+                                      // messages, then two mbarriers (byte offset in dynamic smem)
   const float* alpha;              // NMS weights [nms_iters][nms_L]
   const float* beta;
   int nms_iters;
@@ -216,7 +218,7 @@ int state_flood_threads();
 const void* state_flood_kernel_ptr(int dcmax, bool all_smem);
 int decode_dcmax_bucket(int max_dc);
 int layered_dcmax_bucket(int max_dc);
-const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt);
+const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt, bool stage = false);
 size_t layered_smem_bytes(int smem_app_floats, int bitmap_words, int parity_words);
 size_t decode_smem_bytes(int smem_app_floats, int bitmap_words);
 

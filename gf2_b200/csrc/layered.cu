@@ -38,6 +38,8 @@
 // APP update is v2c + c2v_new.
 #include <cuda_fp16.h>
 
+#include <type_traits>
+
 #include "internal.h"
 #include "numeric.cuh"
 
@@ -77,6 +79,76 @@ template <>
 __device__ __forceinline__ void st_msg<1>(__half* p, int s, float v) {
   __stcs((unsigned short*)p + s, __half_as_ushort(__float2half_rn(v)));
 }
+
+// Old messages of one check: slot i at p[i * nchk] of the (streamed) global
+// message array, or at a shared-memory stage that a TMA copy filled.
+template <int MSG16>
+struct GlobalOld {
+  const typename MsgIO<MSG16>::T* p;  // c2v + edge0 + t
+  int nchk;
+  __device__ __forceinline__ float ld(int i) const { return ld_msg<MSG16>(p, i * nchk); }
+};
+template <int MSG16>
+struct SharedOld {
+  uint32_t a;       // shared address of slot 0 of the check
+  uint32_t stride;  // bytes between slots (nchk messages)
+  __device__ __forceinline__ float ld(int i) const {
+    if constexpr (MSG16) {
+      unsigned short h;
+      asm volatile("ld.shared.u16 %0, [%1];" : "=h"(h) : "r"(a + i * stride));
+      return __half2float(__ushort_as_half(h));
+    } else {
+      float x;
+      asm volatile("ld.shared.f32 %0, [%1];" : "=f"(x) : "r"(a + i * stride));
+      return x;
+    }
+  }
+};
+
+// TMA (bulk copy engine) helpers: a 1-D global -> shared copy whose bytes an
+// mbarrier counts, and bounded waits on the mbarrier's phase.
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Every wait is bounded: a copy that never lands makes the kernel report an
+// error and stop instead of spinning forever.
+constexpr int kStageWaitLimit = 1 << 22;
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  for (int k = 0; k < kStageWaitLimit; k++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load_1d(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+// Shared-memory message stage of the layered kernel: two buffers of one row
+// group's messages each (the row group being decoded and the next one, whose
+// old messages a TMA copy brings in meanwhile) and one mbarrier per buffer.
+struct Stage {
+  uint32_t buf;     // shared address of buffer 0; buffer b at buf + b * bytes
+  uint32_t bytes;   // bytes per buffer
+  uint32_t bar;     // shared address of mbarrier 0 (mbarrier b at bar + 8 b)
+  uint32_t phase;   // bit b: parity of the next completion of mbarrier b
+  uint32_t step;    // row groups decoded so far (buffer of a row group = step & 1)
+  bool pending;     // a copy was issued that no row group has consumed yet
+};
 
 struct LayerSmem {
   uint32_t* bitmap;   // hard decisions, n bits
@@ -122,9 +194,9 @@ __device__ __forceinline__ void app_put(float* app, int v, bool old_neg, float n
 // site).  Same arithmetic as the general path of bp_layered_kernel.  PART:
 // the row group has d < D slots; slots d..D-1 take a neutral input (e = 0,
 // positive, as the general path's missing edges) and store nothing.
-template <int MSG16, int D, bool PART>
+template <int MSG16, int D, bool PART, class OM>
 __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
-                                             typename MsgIO<MSG16>::T* __restrict__ c2v, bool first,
+                                             typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om, bool first,
                                              const LayerSmem& S, const int2* __restrict__ vg,
                                              const int* __restrict__ ci, int vgs, int d) {
   typedef MsgIO<MSG16> IO;
@@ -137,7 +209,7 @@ __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t,
   if (!first) {
 #pragma unroll
     for (int i = 0; i < D; i++)
-      if (!PART || i < d) x[i] = __fsub_rn(x[i], ld_msg<MSG16>(c2v, s0 + i * nchk));
+      if (!PART || i < d) x[i] = __fsub_rn(x[i], om.ld(i));
   }
   float N = 1.0f, Dp = 1.0f;
 #pragma unroll
@@ -179,9 +251,9 @@ __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t,
 // slot of each run adds the run's deltas to its variable in slot order
 // (ascending circulant shift).  The result is the one of the slot-by-slot
 // update with a barrier between the slots of a block, with one barrier.
-template <int MSG16, int D, bool PART>
+template <int MSG16, int D, bool PART, class OM>
 __device__ __forceinline__ void spa_fast_rep_a(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
-                                               typename MsgIO<MSG16>::T* __restrict__ c2v, bool first,
+                                               typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om, bool first,
                                                uint32_t sync, float* dbuf, const LayerSmem& S,
                                                const int2* __restrict__ vg, const int* __restrict__ ci, int vgs,
                                                int d) {
@@ -193,7 +265,7 @@ __device__ __forceinline__ void spa_fast_rep_a(const int2* __restrict__ sd, int 
 #pragma unroll
   for (int i = 0; i < D; i++) {
     if (!PART || i < d) {
-      const float o = first ? 0.0f : ld_msg<MSG16>(c2v, s0 + i * nchk);
+      const float o = first ? 0.0f : om.ld(i);
       dbuf[i * nchk + t] = o;
       if (!first) x[i] = __fsub_rn(x[i], o);
     }
@@ -258,9 +330,10 @@ __device__ __forceinline__ void spa_fast_rep_b(const int2* __restrict__ sd, int 
 // message rounded through the message type, APP + (c2v_new - c2v_old)), so
 // results are bit-identical.  PART: the row group has d < D slots; slots
 // d..D-1 are absent (no load, no store).
-template <int ALGO, int MSG16, int D, bool PART>
+template <int ALGO, int MSG16, int D, bool PART, class OM>
 __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
-                                       typename MsgIO<MSG16>::T* __restrict__ c2v, bool first, float al, float be,
+                                       typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om, bool first,
+                                       float al, float be,
                                        const LayerSmem& S, const int2* __restrict__ vg, const int* __restrict__ ci,
                                        int vgs, int d) {
   typedef MsgIO<MSG16> IO;
@@ -268,7 +341,7 @@ __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int n
 #pragma unroll
   for (int i = 0; i < D; i++) ap[i] = (!PART || i < d) ? app[slot_u(__ldg(&sd[i]), t, nchk)] : 0.0f;
 #pragma unroll
-  for (int i = 0; i < D; i++) o[i] = (first || (PART && i >= d)) ? 0.0f : ld_msg<MSG16>(c2v, s0 + i * nchk);
+  for (int i = 0; i < D; i++) o[i] = (first || (PART && i >= d)) ? 0.0f : om.ld(i);
   float m1 = __int_as_float(0x7f800000), m2 = m1;
   int i1 = -1;
   uint32_t neg = 0, apneg = 0;
@@ -318,9 +391,10 @@ __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int n
 // B (spa_fast_rep_b, after one barrier), the other slots update their unique
 // variable now.  Same additions in the same order as the slot-by-slot general
 // path, so results are bit-identical.
-template <int ALGO, int MSG16, int D, bool PART>
+template <int ALGO, int MSG16, int D, bool PART, class OM>
 __device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
-                                         typename MsgIO<MSG16>::T* __restrict__ c2v, bool first, float al, float be,
+                                         typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om, bool first,
+                                         float al, float be,
                                          uint32_t sync, float* dbuf, const LayerSmem& S,
                                          const int2* __restrict__ vg, const int* __restrict__ ci, int vgs, int d) {
   typedef MsgIO<MSG16> IO;
@@ -329,7 +403,7 @@ __device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int
 #pragma unroll
   for (int i = 0; i < D; i++) ap[i] = (!PART || i < d) ? app[slot_u(__ldg(&sd[i]), t, nchk)] : 0.0f;
 #pragma unroll
-  for (int i = 0; i < D; i++) o[i] = (first || (PART && i >= d)) ? 0.0f : ld_msg<MSG16>(c2v, s0 + i * nchk);
+  for (int i = 0; i < D; i++) o[i] = (first || (PART && i >= d)) ? 0.0f : om.ld(i);
   float m1 = __int_as_float(0x7f800000), m2 = m1;
   int i1 = -1;
   uint32_t neg = 0;
@@ -372,10 +446,19 @@ __device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int
 
 // Iterations of one frame with row groups of at most DCMAX slots; returns the
 // iteration count and whether the syndrome test passed at an early stop.
-template <int ALGO, int MSG16, int DCMAX>
+//
+// STG: the old messages of each row group are read from a shared-memory stage
+// instead of global memory.  While row group g is decoded, one thread has a
+// TMA bulk copy bring the old messages of the next row group (of the next
+// iteration after the last row group) into the other buffer; every thread
+// waits on that buffer's mbarrier (bounded) before reading it.  New messages
+// are stored to global memory by the threads as before, each thread ordering
+// its stores before later TMA reads of them with a proxy fence.  A wait that
+// runs out sets the status word to 2 and *abort, and the kernel returns.
+template <int ALGO, int MSG16, int DCMAX, bool STG>
 __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const DevCode& C, float* app,
                                                    typename MsgIO<MSG16>::T* __restrict__ c2v, const LayerSmem& S,
-                                                   int maxit, int& it, int& converged) {
+                                                   int maxit, int& it, int& converged, Stage& stg, int* abort) {
   typedef MsgIO<MSG16> IO;
   const int tid = threadIdx.x, vgs = C.vgs, ncg = C.ncg;
   const int4* __restrict__ cgp = C.cg;
@@ -389,6 +472,7 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
   converged = 0;
   // fused row paths: every algorithm but the exact sum-product
   constexpr bool kFused = (ALGO == L_SPA_FAST || ALGO == L_MS || ALGO == L_NMS) && DCMAX <= 22;
+  constexpr int kMsgBytes = MSG16 ? 2 : 4;
   for (;;) {
     const int tw = (a.nms_iters > 0) ? min(it, a.nms_iters - 1) : 0;
     const bool first = (it == 0);
@@ -400,6 +484,35 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
       const int t = act ? tid : 0;
       const int s0 = G.w + t;
       const int2* __restrict__ sd = sdesc + spcg[g].w;
+      typedef typename std::conditional<STG, SharedOld<MSG16>, GlobalOld<MSG16>>::type OM;
+      OM om;
+      if constexpr (STG) {
+        const uint32_t b = stg.step & 1u;
+        if (!first) {  // this row group's old messages: wait for the copy into buffer b
+          if (!mbar_wait_bounded(stg.bar + 8 * b, (stg.phase >> b) & 1u)) {
+            *abort = 1;
+            atomicExch(a.status, 2);
+          }
+          stg.phase ^= 1u << b;
+          stg.pending = false;
+        }
+        // the next row group's old messages (the next iteration's first after the last)
+        const bool issue = (g + 1 < ncg) ? !first : (it + 1 < maxit);
+        if (issue) {
+          const int gn = (g + 1 < ncg) ? g + 1 : 0;
+          if (tid == 0) {
+            const int4 Gn = cgp[gn];
+            const uint32_t nb = b ^ 1u, bytes = (uint32_t)(Gn.z * Gn.y * kMsgBytes);
+            fence_proxy_async_shared();  // the buffer's last reads (previous row group) before the copy
+            mbar_expect_tx(stg.bar + 8 * nb, bytes);
+            tma_load_1d(stg.buf + nb * stg.bytes, c2v + Gn.w, bytes, stg.bar + 8 * nb);
+          }
+          stg.pending = true;
+        }
+        om = OM{stg.buf + b * stg.bytes + (uint32_t)(t * kMsgBytes), (uint32_t)(nchk * kMsgBytes)};
+      } else {
+        om = OM{c2v + s0, nchk};
+      }
       int vv[DCMAX];
       float ap[DCMAX], o[DCMAX], w[DCMAX];
       uint32_t real = 0, neg = 0, apneg = 0;
@@ -418,17 +531,17 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
         if (act) {
           if constexpr (ALGO == L_SPA_FAST) {
             if (d == DCMAX)
-              spa_fast_rep_a<MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, first, sync, S.dbuf, S, vg, vg_chk, vgs,
+              spa_fast_rep_a<MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, om, first, sync, S.dbuf, S, vg, vg_chk, vgs,
                                                   d);
             else
-              spa_fast_rep_a<MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, first, sync, S.dbuf, S, vg, vg_chk, vgs,
+              spa_fast_rep_a<MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, om, first, sync, S.dbuf, S, vg, vg_chk, vgs,
                                                  d);
           } else if constexpr (kFused) {
             if (d == DCMAX)
-              ms_rep_a<ALGO, MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, first, al, be, sync, S.dbuf, S, vg,
+              ms_rep_a<ALGO, MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, om, first, al, be, sync, S.dbuf, S, vg,
                                                   vg_chk, vgs, d);
             else
-              ms_rep_a<ALGO, MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, first, al, be, sync, S.dbuf, S, vg,
+              ms_rep_a<ALGO, MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, om, first, al, be, sync, S.dbuf, S, vg,
                                                  vg_chk, vgs, d);
           }
         }
@@ -437,14 +550,14 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
       } else if (kFused && act && sync == 0 && d >= 2 && d <= DCMAX && ab == 0) {
         if constexpr (ALGO == L_SPA_FAST) {
           if (d == DCMAX)
-            spa_fast_row<MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs, d);
+            spa_fast_row<MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, om, first, S, vg, vg_chk, vgs, d);
           else
-            spa_fast_row<MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, first, S, vg, vg_chk, vgs, d);
+            spa_fast_row<MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, om, first, S, vg, vg_chk, vgs, d);
         } else if constexpr (kFused) {
           if (d == DCMAX)
-            ms_row<ALGO, MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, first, al, be, S, vg, vg_chk, vgs, d);
+            ms_row<ALGO, MSG16, DCMAX, false>(sd, t, nchk, s0, app, c2v, om, first, al, be, S, vg, vg_chk, vgs, d);
           else
-            ms_row<ALGO, MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, first, al, be, S, vg, vg_chk, vgs, d);
+            ms_row<ALGO, MSG16, DCMAX, true>(sd, t, nchk, s0, app, c2v, om, first, al, be, S, vg, vg_chk, vgs, d);
         }
       } else if (act) {
         // 1. indices, 2. all loads, 3. arithmetic
@@ -458,7 +571,7 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
           for (int i = 0; i < DCMAX; i++) o[i] = 0.0f;
         } else {
 #pragma unroll
-          for (int i = 0; i < DCMAX; i++) o[i] = ld_msg<MSG16>(c2v, (i < d) ? s0 + i * nchk : s0);
+          for (int i = 0; i < DCMAX; i++) o[i] = om.ld(i < d ? i : 0);
         }
 #pragma unroll
         for (int i = 0; i < DCMAX; i++) {
@@ -562,7 +675,12 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
           }
         }
       }
+      if constexpr (STG) fence_proxy_async_global();  // this thread's message stores before later TMA reads
       __syncthreads();
+      if constexpr (STG) {
+        stg.step++;
+        if (*abort) return;
+      }
     }
     ++it;
     const int unsat = *S.unsat;
@@ -575,13 +693,14 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
   }
 }
 
-template <int ALGO, int MSG16, int DCMAX, int MAXT, int MINB>
+template <int ALGO, int MSG16, int DCMAX, int MAXT, int MINB, bool STG>
 __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs a) {
   typedef typename MsgIO<MSG16>::T MsgT;
   typedef MsgIO<MSG16> IO;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ long long s_frame;
   __shared__ int s_unsat;
+  __shared__ int s_abort;
   __shared__ DevCode C;
   uint32_t* bitmap = (uint32_t*)smem_raw;
   uint32_t* chkpar = bitmap + a.bitmap_words;
@@ -591,6 +710,18 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
   float* gapp = (float*)(work + a.app_offset);
   const int tid = threadIdx.x, NT = blockDim.x;
   LayerSmem S{bitmap, chkpar, &s_unsat, a.lay_dbuf_floats ? (float*)(smem_raw + a.lay_dbuf_off) : nullptr};
+  Stage stg{};
+  if constexpr (STG) {
+    stg.buf = (uint32_t)__cvta_generic_to_shared(smem_raw + a.lay_stage_off);
+    stg.bytes = (uint32_t)a.lay_stage_bytes;
+    stg.bar = stg.buf + 2 * stg.bytes;
+    if (tid == 0) {
+      mbar_init(stg.bar, 1);
+      mbar_init(stg.bar + 8, 1);
+      s_abort = 0;
+    }
+    __syncthreads();
+  }
 
   for (;;) {
     if (tid == 0) {
@@ -675,19 +806,35 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
 
     int it = 0, converged = 0;
     if constexpr (DCMAX > 0) {
-      layered_iterations<ALGO, MSG16, DCMAX>(a, C, app, c2v, S, maxit, it, converged);
+      layered_iterations<ALGO, MSG16, DCMAX, STG>(a, C, app, c2v, S, maxit, it, converged, stg, &s_abort);
     } else {  // mixed batch: the exact slot count of this frame's code
+#define GF2C_LAY_CASE(D) layered_iterations<ALGO, MSG16, D, STG>(a, C, app, c2v, S, maxit, it, converged, stg, &s_abort)
       switch (C.lay_bucket) {
-        case 7: layered_iterations<ALGO, MSG16, 7>(a, C, app, c2v, S, maxit, it, converged); break;
-        case 9: layered_iterations<ALGO, MSG16, 9>(a, C, app, c2v, S, maxit, it, converged); break;
-        case 10: layered_iterations<ALGO, MSG16, 10>(a, C, app, c2v, S, maxit, it, converged); break;
-        case 11: layered_iterations<ALGO, MSG16, 11>(a, C, app, c2v, S, maxit, it, converged); break;
-        case 13: layered_iterations<ALGO, MSG16, 13>(a, C, app, c2v, S, maxit, it, converged); break;
-        case 14: layered_iterations<ALGO, MSG16, 14>(a, C, app, c2v, S, maxit, it, converged); break;
-        case 18: layered_iterations<ALGO, MSG16, 18>(a, C, app, c2v, S, maxit, it, converged); break;
-        case 19: layered_iterations<ALGO, MSG16, 19>(a, C, app, c2v, S, maxit, it, converged); break;
-        default: layered_iterations<ALGO, MSG16, 22>(a, C, app, c2v, S, maxit, it, converged); break;
+        case 7: GF2C_LAY_CASE(7); break;
+        case 9: GF2C_LAY_CASE(9); break;
+        case 10: GF2C_LAY_CASE(10); break;
+        case 11: GF2C_LAY_CASE(11); break;
+        case 13: GF2C_LAY_CASE(13); break;
+        case 14: GF2C_LAY_CASE(14); break;
+        case 18: GF2C_LAY_CASE(18); break;
+        case 19: GF2C_LAY_CASE(19); break;
+        default: GF2C_LAY_CASE(22); break;
       }
+#undef GF2C_LAY_CASE
+    }
+    if constexpr (STG) {
+      // a copy issued for an iteration that did not run (early stop): let it land
+      if (stg.pending) {
+        const uint32_t b = stg.step & 1u;
+        if (!mbar_wait_bounded(stg.bar + 8 * b, (stg.phase >> b) & 1u)) {
+          s_abort = 1;
+          atomicExch(a.status, 2);
+        }
+        stg.phase ^= 1u << b;
+        stg.pending = false;
+      }
+      __syncthreads();
+      if (s_abort) return;
     }
     if (!converged) converged = (s_unsat == 0);
 
@@ -715,22 +862,24 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
 
 // Row groups of up to 384 checks: one kernel per slot count of the DVB-T2
 // codes (an exact fit wastes no slot and keeps the all-edges fast path).
-template <int ALGO, int MSG16, int MINB>
+// STG: the TMA-staged variant (not for the exact sum-product, which is
+// arithmetic-bound).
+template <int ALGO, int MSG16, int MINB, bool STG>
 static const void* lay_exact(int dcmax) {
   switch (dcmax) {
-    case 7: return (const void*)bp_layered_kernel<ALGO, MSG16, 7, 384, MINB>;
-    case 9: return (const void*)bp_layered_kernel<ALGO, MSG16, 9, 384, MINB>;
-    case 10: return (const void*)bp_layered_kernel<ALGO, MSG16, 10, 384, MINB>;
-    case 11: return (const void*)bp_layered_kernel<ALGO, MSG16, 11, 384, MINB>;
-    case 13: return (const void*)bp_layered_kernel<ALGO, MSG16, 13, 384, MINB>;
-    case 14: return (const void*)bp_layered_kernel<ALGO, MSG16, 14, 384, MINB>;
-    case 18: return (const void*)bp_layered_kernel<ALGO, MSG16, 18, 384, MINB>;
-    case 19: return (const void*)bp_layered_kernel<ALGO, MSG16, 19, 384, MINB>;
-    case 22: return (const void*)bp_layered_kernel<ALGO, MSG16, 22, 384, MINB>;
-    case 26: return (const void*)bp_layered_kernel<ALGO, MSG16, 26, 384, MINB>;
-    case 32: return (const void*)bp_layered_kernel<ALGO, MSG16, 32, 384, MINB>;
+    case 7: return (const void*)bp_layered_kernel<ALGO, MSG16, 7, 384, MINB, STG>;
+    case 9: return (const void*)bp_layered_kernel<ALGO, MSG16, 9, 384, MINB, STG>;
+    case 10: return (const void*)bp_layered_kernel<ALGO, MSG16, 10, 384, MINB, STG>;
+    case 11: return (const void*)bp_layered_kernel<ALGO, MSG16, 11, 384, MINB, STG>;
+    case 13: return (const void*)bp_layered_kernel<ALGO, MSG16, 13, 384, MINB, STG>;
+    case 14: return (const void*)bp_layered_kernel<ALGO, MSG16, 14, 384, MINB, STG>;
+    case 18: return (const void*)bp_layered_kernel<ALGO, MSG16, 18, 384, MINB, STG>;
+    case 19: return (const void*)bp_layered_kernel<ALGO, MSG16, 19, 384, MINB, STG>;
+    case 22: return (const void*)bp_layered_kernel<ALGO, MSG16, 22, 384, MINB, STG>;
+    case 26: return (const void*)bp_layered_kernel<ALGO, MSG16, 26, 384, MINB, STG>;
+    case 32: return (const void*)bp_layered_kernel<ALGO, MSG16, 32, 384, MINB, STG>;
     case 0:  // mixed batches: each frame runs the iterations of its code's exact slot count
-      if constexpr (ALGO == L_SPA_FAST) return (const void*)bp_layered_kernel<ALGO, MSG16, 0, 384, MINB>;
+      if constexpr (ALGO == L_SPA_FAST && !STG) return (const void*)bp_layered_kernel<ALGO, MSG16, 0, 384, MINB, false>;
       return nullptr;
   }
   return nullptr;
@@ -739,19 +888,19 @@ static const void* lay_exact(int dcmax) {
 // Row groups of up to 1024 checks (generic QC codes): coarser slot buckets.
 template <int ALGO, int MSG16>
 static const void* lay_wide(int dcmax) {
-  if (dcmax <= 8) return (const void*)bp_layered_kernel<ALGO, MSG16, 8, 1024, 1>;
-  if (dcmax <= 12) return (const void*)bp_layered_kernel<ALGO, MSG16, 12, 1024, 1>;
-  if (dcmax <= 16) return (const void*)bp_layered_kernel<ALGO, MSG16, 16, 1024, 1>;
-  if (dcmax <= 24) return (const void*)bp_layered_kernel<ALGO, MSG16, 24, 1024, 1>;
-  if (dcmax <= 32) return (const void*)bp_layered_kernel<ALGO, MSG16, 32, 1024, 1>;
+  if (dcmax <= 8) return (const void*)bp_layered_kernel<ALGO, MSG16, 8, 1024, 1, false>;
+  if (dcmax <= 12) return (const void*)bp_layered_kernel<ALGO, MSG16, 12, 1024, 1, false>;
+  if (dcmax <= 16) return (const void*)bp_layered_kernel<ALGO, MSG16, 16, 1024, 1, false>;
+  if (dcmax <= 24) return (const void*)bp_layered_kernel<ALGO, MSG16, 24, 1024, 1, false>;
+  if (dcmax <= 32) return (const void*)bp_layered_kernel<ALGO, MSG16, 32, 1024, 1, false>;
   return nullptr;
 }
 
 template <int ALGO, int MSG16>
-static const void* lay_t(int dcmax, int maxt) {
-  if (maxt > 384) return lay_wide<ALGO, MSG16>(dcmax);
-  if constexpr (ALGO == L_SPA) return lay_exact<ALGO, MSG16, 1>(dcmax);
-  else return lay_exact<ALGO, MSG16, 2>(dcmax);
+static const void* lay_t(int dcmax, int maxt, bool stage) {
+  if (maxt > 384) return stage ? nullptr : lay_wide<ALGO, MSG16>(dcmax);
+  if constexpr (ALGO == L_SPA) return stage ? nullptr : lay_exact<ALGO, MSG16, 1, false>(dcmax);
+  else return stage ? lay_exact<ALGO, MSG16, 2, true>(dcmax) : lay_exact<ALGO, MSG16, 2, false>(dcmax);
 }
 
 int layered_dcmax_bucket(int max_dc) {
@@ -761,12 +910,13 @@ int layered_dcmax_bucket(int max_dc) {
   return -1;
 }
 
-const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt) {
+const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt, bool stage) {
   switch (algo) {
-    case L_MS: return msg16 ? lay_t<L_MS, 1>(dcmax, maxt) : lay_t<L_MS, 0>(dcmax, maxt);
-    case L_SPA: return msg16 ? lay_t<L_SPA, 1>(dcmax, maxt) : lay_t<L_SPA, 0>(dcmax, maxt);
-    case L_NMS: return msg16 ? lay_t<L_NMS, 1>(dcmax, maxt) : lay_t<L_NMS, 0>(dcmax, maxt);
-    case L_SPA_FAST: return msg16 ? lay_t<L_SPA_FAST, 1>(dcmax, maxt) : lay_t<L_SPA_FAST, 0>(dcmax, maxt);
+    case L_MS: return msg16 ? lay_t<L_MS, 1>(dcmax, maxt, stage) : lay_t<L_MS, 0>(dcmax, maxt, stage);
+    case L_SPA: return msg16 ? lay_t<L_SPA, 1>(dcmax, maxt, stage) : lay_t<L_SPA, 0>(dcmax, maxt, stage);
+    case L_NMS: return msg16 ? lay_t<L_NMS, 1>(dcmax, maxt, stage) : lay_t<L_NMS, 0>(dcmax, maxt, stage);
+    case L_SPA_FAST:
+      return msg16 ? lay_t<L_SPA_FAST, 1>(dcmax, maxt, stage) : lay_t<L_SPA_FAST, 0>(dcmax, maxt, stage);
   }
   return nullptr;
 }
