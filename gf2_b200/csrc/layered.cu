@@ -122,13 +122,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Every wait is bounded: a copy that never lands makes the kernel report an
-// error and stop instead of spinning forever.
-constexpr int kStageWaitLimit = 1 << 22;
+// Every wait is bounded in time (the global nanosecond timer): a copy that
+// never lands makes the kernel report an error and stop instead of spinning.
+constexpr unsigned long long kStageWaitNs = 2000000000ull;
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-  for (int k = 0; k < kStageWaitLimit; k++)
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
     if (mbar_try_wait(bar, parity)) return true;
-  return false;
+    if (global_ns() - t0 > kStageWaitNs) return false;
+  }
 }
 __device__ __forceinline__ void tma_load_1d(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
