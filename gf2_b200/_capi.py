@@ -34,7 +34,7 @@ EXPORTS = [
     "gf2c_code_destroy", "gf2c_code_dims", "gf2c_code_csr", "gf2c_syndrome_batch",
     "gf2c_encode_batch", "gf2c_channel_awgn", "gf2c_sigma2_from_ebn0",
     "gf2c_decoder_create", "gf2c_decoder_create_multi", "gf2c_decoder_destroy",
-    "gf2c_decode_batch", "gf2c_decode_mixed", "gf2c_decoder_last_launches", "gf2c_decode_batch_noalloc",
+    "gf2c_decode_batch", "gf2c_decode_batch_fallback", "gf2c_decode_mixed", "gf2c_decoder_last_launches", "gf2c_decode_batch_noalloc",
     "gf2c_judge_spa64",
     "gf2c_nms_trainer_create", "gf2c_nms_trainer_destroy", "gf2c_nms_trainer_layers", "gf2c_nms_trainer_set_schedule", "gf2c_nms_loss_grad",
     "gf2c_adam_step", "gf2c_count_errors",
@@ -96,6 +96,7 @@ def _load():
     L.gf2c_decoder_create_multi.argtypes = [_vp, _i32, ctypes.POINTER(DecoderOpts), ctypes.POINTER(_vp)]
     L.gf2c_decoder_destroy.argtypes = [_vp]
     L.gf2c_decode_batch.argtypes = [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _vp]
+    L.gf2c_decode_batch_fallback.argtypes = [_vp, _vp, _vp, _i64, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp]
     L.gf2c_decode_mixed.argtypes = [_vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _vp]
     L.gf2c_decoder_last_launches.argtypes = [_vp, ctypes.POINTER(_i32)]
     L.gf2c_decode_batch_noalloc.argtypes = [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp]

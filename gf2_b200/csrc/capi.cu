@@ -85,6 +85,8 @@ struct gf2c_decoder {
   DevBuf d_rank, d_order;
   // single-code batches, hardest frames first: per-frame keys and order (one pair per stream slot)
   DevBuf d_key[2], d_korder[2];
+  // fallback decoding: the frames this decoder left failing (list and count)
+  DevBuf fb_list, fb_count;
   ~gf2c_decoder() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     if (gstream) {
@@ -711,6 +713,59 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
   if (syndrome_ok) GF2C_CUDA(cudaMemcpyAsync(syndrome_ok, dec->s_so.p, frames, cudaMemcpyDeviceToHost, st));
   if (beliefs) GF2C_CUDA(cudaMemcpyAsync(beliefs, dec->s_bel.p, bl, cudaMemcpyDeviceToHost, st));
   return check_status(dec, st);
+}
+
+int gf2c_decode_batch_fallback(gf2c_decoder* primary, gf2c_decoder* fallback, const float* llr, int64_t frames,
+                               int32_t max_iter_primary, int32_t max_iter_fallback, uint64_t* msg_bits,
+                               int32_t* iterations, uint8_t* converged, uint8_t* syndrome_ok,
+                               int64_t* fallback_count, void* stream) {
+  if (!primary || !fallback || frames < 0 || max_iter_primary < 0 || max_iter_fallback <= 0 || (frames > 0 && !llr))
+    return set_error(GF2C_ERR_INVALID_ARG, "bad arguments");
+  if (primary->codes.size() != 1 || fallback->codes.size() != 1 ||
+      primary->codes[0]->h->serial != fallback->codes[0]->h->serial)
+    return set_error(GF2C_ERR_INVALID_ARG, "both decoders must decode the same single code");
+  if (fallback->opts.schedule != GF2C_SCHED_LAYERED)
+    return set_error(GF2C_ERR_UNSUPPORTED, "the fallback decoder must use the layered schedule");
+  if (frames == 0) return GF2C_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  uint8_t* so = syndrome_ok;
+  if (!so) {
+    if ((rc = primary->s_so.ensure((size_t)frames))) return rc;
+    so = (uint8_t*)primary->s_so.p;
+  }
+  if ((rc = primary->fb_list.ensure((size_t)frames * 8)) || (rc = primary->fb_count.ensure(64))) return rc;
+  // 1. the primary decoder on every frame
+  DecodeArgs a{};
+  a.max_iter = max_iter_primary;
+  a.llr = llr;
+  a.msg = msg_bits;
+  a.iters = iterations;
+  a.conv = converged;
+  a.synd_ok = so;
+  int extra = 0;
+  if ((rc = key_order(primary, a, frames, st, 0, extra))) return rc;
+  if ((rc = launch_decoder(primary, a, frames, st))) return rc;
+  const int launches = primary->last_launches + extra;
+  // 2. the frames it left failing, listed on the device
+  long long* cnt = (long long*)primary->fb_count.p;
+  GF2C_CUDA(launch_failed_list(so, frames, (int64_t*)primary->fb_list.p, cnt, st));
+  // 3. the fallback decoder on the listed frames (count read on the device)
+  DecodeArgs b{};
+  b.max_iter = max_iter_fallback;
+  b.llr = llr;
+  b.msg = msg_bits;
+  b.iters = iterations;
+  b.conv = converged;
+  b.synd_ok = so;
+  b.order = (const int64_t*)primary->fb_list.p;
+  b.frames_dev = cnt;
+  b.iters_add = max_iter_primary;
+  if ((rc = launch_decoder(fallback, b, frames, st))) return rc;
+  if (fallback_count)
+    GF2C_CUDA(cudaMemcpyAsync(fallback_count, cnt, sizeof(long long), cudaMemcpyDeviceToDevice, st));
+  primary->last_launches = launches + 2;
+  return GF2C_OK;
 }
 
 int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_offset, const int32_t* code_id,

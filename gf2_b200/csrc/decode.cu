@@ -454,6 +454,43 @@ cudaError_t launch_mixed_order(const int32_t* code_id, int64_t frames, const int
   return cudaGetLastError();
 }
 
+// The frames a first decoder left with a failing syndrome, for the fallback
+// pass: the same block-wide stable compaction (ballot + popc per warp, warp
+// totals in shared memory), ascending frame index, count written last.
+__global__ void __launch_bounds__(1024) failed_list_kernel(const uint8_t* __restrict__ synd_ok, int64_t frames,
+                                                           int64_t* __restrict__ list, long long* __restrict__ count) {
+  __shared__ int s_warp[32];
+  __shared__ long long s_pos;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  if (tid == 0) s_pos = 0;
+  __syncthreads();
+  for (long long base = 0; base < frames; base += blockDim.x) {
+    const long long f = base + tid;
+    const bool hit = f < frames && synd_ok[f] == 0;
+    const unsigned b = __ballot_sync(0xffffffffu, hit);
+    if (lane == 0) s_warp[wid] = __popc(b);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < nw; w++) {
+      const int x = s_warp[w];
+      before += (w < wid) ? x : 0;
+      total += x;
+    }
+    const long long p0 = s_pos;
+    if (hit) list[p0 + before + __popc(b & ((1u << lane) - 1u))] = f;
+    __syncthreads();
+    if (tid == 0) s_pos = p0 + total;
+    __syncthreads();
+  }
+  if (tid == 0) *count = s_pos;
+}
+
+cudaError_t launch_failed_list(const uint8_t* synd_ok, int64_t frames, int64_t* list, long long* count,
+                               cudaStream_t st) {
+  failed_list_kernel<<<1, 1024, 0, st>>>(synd_ok, frames, list, count);
+  return cudaGetLastError();
+}
+
 // Sum of |LLR| of each frame (one CTA per frame, a fixed summation order).
 __global__ void __launch_bounds__(256) frame_key_kernel(const float* __restrict__ llr, int n,
                                                         float* __restrict__ key) {

@@ -180,6 +180,9 @@ struct DecodeArgs {
   uint8_t* synd_ok;
   float* beliefs;                  // nullable
   long long frames;
+  const long long* frames_dev;     // nullable: number of queue entries (order[0..*frames_dev)) in device
+                                   // memory; frames then only bounds the frame indices
+  int iters_add;                   // added to every reported iteration count
   unsigned long long* queue;       // work counter, zero at launch
   char* work;                      // per-CTA workspace
   long long work_stride;           // bytes per CTA
@@ -213,6 +216,10 @@ cudaError_t launch_mixed_order(const int32_t* code_id, int64_t frames, const int
 // |LLR| per frame (ties by frame index).  frames <= kKeyOrderMax; key: frames floats.
 constexpr int kKeyOrderMax = 16384;
 cudaError_t launch_key_order(const float* llr, int n, int64_t frames, float* key, int64_t* order, cudaStream_t st);
+// Frames whose syndrome check failed (syndrome_ok[f] == 0), ascending, into
+// list; their number into *count (one CTA, device memory only).
+cudaError_t launch_failed_list(const uint8_t* syndrome_ok, int64_t frames, int64_t* list, long long* count,
+                               cudaStream_t st);
 int state_dcmax_bucket(int max_dc);
 int state_flood_threads();
 const void* state_flood_kernel_ptr(int dcmax, bool all_smem);

@@ -734,12 +734,13 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
   for (;;) {
     if (tid == 0) {
       const long long q = (long long)atomicAdd(a.queue, 1ull);
-      s_frame = (a.order != nullptr && q < a.frames) ? a.order[q] : q;
+      const long long nq = a.frames_dev ? *a.frames_dev : a.frames;  // queue entries
+      s_frame = (q < nq) ? (a.order != nullptr ? a.order[q] : q) : -1;
       s_unsat = 0;
     }
     __syncthreads();
     const long long f = s_frame;
-    if (f >= a.frames) break;
+    if (f < 0 || f >= a.frames) break;
     const int cid = a.code_id ? a.code_id[f] : 0;
     if (cid < 0 || cid >= a.ncodes) {
       if (tid == 0) {
@@ -860,7 +861,7 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
     if (bo)
       for (int u = tid; u < n; u += NT) bo[u2v ? __ldg(&u2v[u]) : u] = app[u];
     if (tid == 0) {
-      if (a.iters) a.iters[f] = it;
+      if (a.iters) a.iters[f] = it + a.iters_add;
       if (a.conv) a.conv[f] = (uint8_t)converged;
       if (a.synd_ok) a.synd_ok[f] = (uint8_t)converged;
     }

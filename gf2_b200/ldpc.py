@@ -486,6 +486,29 @@ class LdpcDecoder:
                                         _ptr(out.get("beliefs")), C.MEM_DEVICE, _stream_ptr(st)))
         return out
 
+    def decode_with_fallback(self, fallback, llr, max_iterations, fallback_iterations, out=None, stream=None):
+        """This decoder on every frame of a device batch, then `fallback` (a
+        layered decoder of the same code) on the frames whose syndrome still
+        fails, all on the device (gf2c_decode_batch_fallback).  Returns a dict
+        of device tensors; fallback_count [1] int64 = frames re-decoded."""
+        import torch
+        if llr.dtype != torch.float32 or not llr.is_cuda or llr.dim() != 2 or llr.shape[1] != self.n():
+            raise ValueError("llr must be a CUDA float32 tensor [frames, n]")
+        llr = llr.contiguous()
+        F, dev = llr.shape[0], llr.device
+        if out is None:
+            out = dict(msg=torch.zeros((F, words(self.k())), dtype=torch.int64, device=dev),
+                       iters=torch.zeros(F, dtype=torch.int32, device=dev),
+                       conv=torch.zeros(F, dtype=torch.uint8, device=dev),
+                       synd_ok=torch.zeros(F, dtype=torch.uint8, device=dev),
+                       fallback_count=torch.zeros(1, dtype=torch.int64, device=dev))
+        st = stream or torch.cuda.current_stream(dev)
+        C.check(C.lib.gf2c_decode_batch_fallback(self._h, fallback._h, _ptr(llr), F, int(max_iterations),
+                                                 int(fallback_iterations), _ptr(out["msg"]), _ptr(out["iters"]),
+                                                 _ptr(out["conv"]), _ptr(out["synd_ok"]),
+                                                 _ptr(out["fallback_count"]), _stream_ptr(st)))
+        return out
+
     def decode_iterative(self, llrs, max_iterations):
         """IterativeSoftDecoder::decode_iterative (traits.rs:335, core.rs:889-938)."""
         a = _llr_array(llrs, self.n())

@@ -177,6 +177,22 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
                       uint64_t* msg_bits, int32_t* iterations, uint8_t* converged,
                       uint8_t* syndrome_ok, float* beliefs, int32_t mem, void* stream);
 
+/* A decoder with a fallback, on the device -- no counterpart in the reference
+ * (its decode_batch, core.rs:729-756, runs one decoder).  `primary` (e.g. the
+ * learned min-sum decoder) decodes every frame with max_iter_primary
+ * iterations; a small kernel lists the frames whose syndrome still fails, and
+ * `fallback` (e.g. sum-product, layered schedule) decodes those frames again
+ * from their LLRs with max_iter_fallback iterations, its results replacing
+ * theirs (iterations = max_iter_primary + the fallback's count).  The list
+ * and its length stay on the device: no host synchronisation between the
+ * passes.  fallback_count (nullable, device int64): frames re-decoded.
+ * Both decoders must decode the same code.  All pointers are device memory;
+ * asynchronous on `stream`; 3 or 5 kernel launches. */
+int gf2c_decode_batch_fallback(gf2c_decoder* primary, gf2c_decoder* fallback, const float* llr, int64_t frames,
+                               int32_t max_iter_primary, int32_t max_iter_fallback, uint64_t* msg_bits,
+                               int32_t* iterations, uint8_t* converged, uint8_t* syndrome_ok,
+                               int64_t* fallback_count, void* stream);
+
 /* Mixed batch in one persistent launch: frame f uses code code_id[f] (index into the
  * codes given at creation), reads n[code] LLRs at llr + llr_offset[f], writes
  * ceil(k/64) words at msg_bits + msg_offset[f] (both in elements), and has its own
