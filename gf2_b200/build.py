@@ -13,8 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libgf2cuda.so")
-SOURCES = ["capi.cu", "code_host.cpp", "decode.cu", "layered.cu", "encode_channel.cu", "learned.cu", "noalloc.cu", "spa64.cu", "state_flood.cu", "bch.cu", "gf2io.cpp", "dense_encode.cu"]
-HEADERS = ["internal.h", "numeric.cuh", "dvbt2_tables.h", "../../include/gf2cuda.h"]
+SOURCES = ["capi.cu", "code_host.cpp", "decode.cu", "layered.cu", "layered_sfu16.cu", "layered_sfu32.cu", "layered_nms16.cu", "layered_nms32.cu", "layered_spa16.cu", "layered_spa32.cu", "encode_channel.cu", "learned.cu", "noalloc.cu", "spa64.cu", "state_flood.cu", "bch.cu", "gf2io.cpp", "dense_encode.cu"]
+HEADERS = ["internal.h", "numeric.cuh", "layered_impl.cuh", "dvbt2_tables.h", "../../include/gf2cuda.h"]
 
 
 def nvcc():

@@ -360,13 +360,31 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
     GF2C_CUDA(cudaMemcpy(d->beta.p, opts->nms_beta, nb, cudaMemcpyHostToDevice));
   }
 
+  // Layered min-sum runs on the normalised / offset min-sum kernels with one
+  // weight pair alpha = 1, beta = 0 (bit-identical messages: 1 * max(m - 0, 0) = m).
+  if (o.schedule == GF2C_SCHED_LAYERED && o.algorithm == GF2C_ALGO_MINSUM) {
+    const float one = 1.0f, zero = 0.0f;
+    d->nms_L = 1;
+    d->nms_iters = 1;
+    if ((rc = d->alpha.ensure(sizeof(float))) || (rc = d->beta.ensure(sizeof(float)))) return rc;
+    GF2C_CUDA(cudaMemcpy(d->alpha.p, &one, sizeof(float), cudaMemcpyHostToDevice));
+    GF2C_CUDA(cudaMemcpy(d->beta.p, &zero, sizeof(float), cudaMemcpyHostToDevice));
+  }
+
   // launch shape
   int sms = 148;
   GF2C_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->dev));
   int threads = o.threads_per_block;
   if (threads == 0) threads = layered ? ((d->max_nchk + 31) / 32) * 32 : 512;
-  if (layered && threads < d->max_nchk)
-    return set_error(GF2C_ERR_INVALID_ARG, "layered schedule needs threads_per_block >= row group size");
+  // Layered: one thread per check of a row group, or (several checks per
+  // thread, more frames in flight per SM) 192 / 128 threads for one code with
+  // FP16 messages and a fused-row algorithm, on the TMA-staged kernel.
+  const bool multi = layered && threads < d->max_nchk;
+  if (multi && !((threads == 192 || threads == 128) && d->codes.size() == 1 && o.msg_dtype == GF2C_MSG_F16 &&
+                 o.algorithm != GF2C_ALGO_SPA && d->max_nchk <= 384))
+    return set_error(GF2C_ERR_INVALID_ARG,
+                     "layered schedule needs threads_per_block >= row group size (or 192 / 128 threads for one "
+                     "DVB-T2 code, FP16 messages, min-sum / NMS / SFU sum-product)");
   threads = std::max(threads, 32);
   d->threads = threads;
   d->bitmap_words = (d->max_n + 31) / 32;
@@ -441,10 +459,13 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
     d->threads = threads;
     d->state_flood = true;
   }
-  if (!d->kernel) return set_error(GF2C_ERR_UNSUPPORTED, "no decode kernel for this configuration");
+  if (!d->kernel && !multi) return set_error(GF2C_ERR_UNSUPPORTED, "no decode kernel for this configuration");
   if (!layered && !d->state_flood && threads > 512)
     return set_error(GF2C_ERR_INVALID_ARG, "flooding schedule: threads_per_block must be <= 512");
-  if (d->lay_dbuf_floats > 0) {
+  if (multi && d->lay_dbuf_floats > 0) {
+    // several checks per thread: the delta buffer is required
+    d->smem = (size_t)d->lay_dbuf_off + (size_t)d->lay_dbuf_floats * 4;
+  } else if (d->lay_dbuf_floats > 0) {
     int optin = 0, occ0 = 0, occ1 = 0;
     GF2C_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->dev));
     const size_t with = (size_t)d->lay_dbuf_off + (size_t)d->lay_dbuf_floats * 4;
@@ -479,11 +500,13 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
     GF2C_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->dev));
     const size_t off = (d->smem + 15) & ~(size_t)15, with = off + 2 * mx + 16;
     if (k && with <= (size_t)optin) {
-      GF2C_CUDA(cudaFuncSetAttribute(d->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d->smem));
-      GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, d->kernel, threads, d->smem));
+      if (d->kernel) {
+        GF2C_CUDA(cudaFuncSetAttribute(d->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d->smem));
+        GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, d->kernel, threads, d->smem));
+      }
       GF2C_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)with));
       GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, k, threads, with));
-      if (occ1 > 0 && (occ1 >= occ0 || std::getenv("GF2C_FORCE_STAGE"))) {
+      if (occ1 > 0 && (occ1 >= occ0 || !d->kernel || std::getenv("GF2C_FORCE_STAGE"))) {
         d->kernel = k;
         d->smem = with;
         d->lay_stage_off = (int)off;
@@ -491,6 +514,9 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
       }
     }
   }
+  if (!d->kernel)
+    return set_error(GF2C_ERR_UNSUPPORTED, "no decode kernel for this configuration (several checks per thread "
+                                          "need the staged kernel: 16-byte aligned row groups, >= 3 row groups)");
   GF2C_CUDA(cudaFuncSetAttribute(d->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d->smem));
   int occ = 0;
   GF2C_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, d->kernel, threads, d->smem));
@@ -538,7 +564,10 @@ static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaSt
   a.lay_stage_bytes = d->lay_stage_bytes;
   a.alpha = (const float*)d->alpha.p;
   a.beta = (const float*)d->beta.p;
-  a.nms_iters = d->opts.algorithm == GF2C_ALGO_NMS ? d->nms_iters : 0;
+  a.nms_iters = (d->opts.algorithm == GF2C_ALGO_NMS ||
+                 (d->opts.algorithm == GF2C_ALGO_MINSUM && d->opts.schedule == GF2C_SCHED_LAYERED))
+                    ? d->nms_iters
+                    : 0;
   a.nms_L = d->nms_L;
   a.early_stop = d->opts.early_stop;
   a.status = (int*)d->status.p;

@@ -1,0 +1,8 @@
+// gf2cuda layered-schedule kernels: normalised / offset min-sum (GF2C_ALGO_NMS, and GF2C_ALGO_MINSUM as alpha 1, beta 0), FP16 messages.
+#include "layered_impl.cuh"
+
+namespace gf2c {
+
+const void* layered_nms16_kernel(int dcmax, int maxt, bool stage) { return lay_t<L_NMS, 1>(dcmax, maxt, stage); }
+
+}  // namespace gf2c

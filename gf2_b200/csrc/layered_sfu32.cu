@@ -1,0 +1,8 @@
+// gf2cuda layered-schedule kernels: sum-product on the SFU (GF2C_ALGO_SPA_FAST), FP32 messages.
+#include "layered_impl.cuh"
+
+namespace gf2c {
+
+const void* layered_sfu32_kernel(int dcmax, int maxt, bool stage) { return lay_t<L_SPA_FAST, 0>(dcmax, maxt, stage); }
+
+}  // namespace gf2c
