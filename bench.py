@@ -7,7 +7,7 @@ the library's channel kernel (info bits, encoder, BPSK, AWGN, LLR = 2y/sigma^2),
 standing in for the reference's AWGN simulation inputs.
 
 Workloads (one "step" = one decode of the whole batch):
-  c2 (default)  DVB-T2 normal rate 3/5 (n=64800, k=38880), 4096 frames,
+  c2            DVB-T2 normal rate 3/5 (n=64800, k=38880), 4096 frames,
                 layered sum-product (SFU), messages stored FP16 / computed FP32,
                 max 50 iterations with syndrome early stop; frame f at
                 Eb/N0 = 0.6 + 0.1 (f mod 9) dB (the 0.6..1.4 dB sweep in one batch).
@@ -22,7 +22,7 @@ Workloads (one "step" = one decode of the whole batch):
                 reference's AwgnChannel::shannon_limit(k/n)), per-frame budget
                 ~ U{10..50}; one persistent launch replayed from a CUDA graph,
                 launch shape from the autotuner; layered sum-product (SFU), FP16.
-  c5            DVB-T2 normal 2/3 (n=64800, k=43200), 65536 frames, learned
+  c5 (default)  DVB-T2 normal 2/3 (n=64800, k=43200), 65536 frames, learned
                 normalised/offset min-sum (per-iteration, per-row-group weights
                 trained on the GPU by the library's layered forward / backward
                 kernels, gf2_b200/weights), 10 layered iterations, FP16 messages,
@@ -105,7 +105,7 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="c2", choices=WORKLOADS)
+    p.add_argument("--workload", default="c5", choices=WORKLOADS)
     p.add_argument("--frames", type=int, default=0, help="override frames per rank (profiling)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -276,10 +276,17 @@ class SingleCode:
         s2 = np.array([g.sigma2_from_ebn0(pts[f % len(pts)], self.code.rate()) for f in range(self.frames)])
         _, _, self.llr = g.awgn_frames(self.code, 1, rank * self.frames, self.frames, s2, device=dev,
                                        want_info=False, want_cw=False)
-        self.dec = g.LdpcDecoder(self.code, algorithm=w["algo"], schedule=w["sched"],
-                                 msg_dtype=g.MSG_F16 if w["msg16"] else g.MSG_F32)
+        msg = g.MSG_F16 if w["msg16"] else g.MSG_F32
+        shape = (0, 0)
+        if w["sched"] == g.SCHED_LAYERED:
+            from gf2_b200 import autotune
+            sample = self.llr[:min(2048, self.frames)]
+            shape, _ = autotune.tune([self.code], w["algo"], w["sched"], msg,
+                                     lambda d: d.decode_tensors(sample, w["max_iter"]))
+        self.dec = g.LdpcDecoder(self.code, algorithm=w["algo"], schedule=w["sched"], msg_dtype=msg,
+                                 threads_per_block=shape[0], blocks_per_sm=shape[1])
         self.out = None
-        self.desc = w["desc"]
+        self.desc = w["desc"] + (f", autotuned launch shape {tuple(shape)}" if w["sched"] == g.SCHED_LAYERED else "")
         self.dtype = "f16 storage / f32 math" if w["msg16"] else "f32"
         self.msg_bytes = 2 if w["msg16"] else 4
 
@@ -462,16 +469,25 @@ class LearnedScale:
         self.info, _, self.llr = g.awgn_frames(self.code, 3, rank * self.frames, self.frames, s2, device=dev,
                                                want_cw=False)
         self.point_of = torch.tensor([f % len(pts) for f in range(self.frames)], device=dev)
-        self.nms = g.LdpcDecoder(self.code, algorithm=g.ALGO_NMS, schedule=g.SCHED_LAYERED, nms_alpha=a,
-                                 nms_beta=b, msg_dtype=g.MSG_F16)
-        self.spa = g.LdpcDecoder(self.code, algorithm=g.ALGO_SPA_FAST, schedule=g.SCHED_LAYERED,
-                                 msg_dtype=g.MSG_F16)
+        # launch shapes of both decoders from the autotuner (timed on the first 8192 frames)
+        from gf2_b200 import autotune
+        sample = self.llr[:min(8192, self.frames)]
+        kw_nms = dict(algorithm=g.ALGO_NMS, schedule=g.SCHED_LAYERED, nms_alpha=a, nms_beta=b, msg_dtype=g.MSG_F16)
+        kw_spa = dict(algorithm=g.ALGO_SPA_FAST, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16)
+        sh_nms, _ = autotune.tune([self.code], g.ALGO_NMS, g.SCHED_LAYERED, g.MSG_F16,
+                                  lambda d: d.decode_tensors(sample, self.T), nms_alpha=a, nms_beta=b)
+        sh_spa, _ = autotune.tune([self.code], g.ALGO_SPA_FAST, g.SCHED_LAYERED, g.MSG_F16,
+                                  lambda d: d.decode_tensors(sample, 50))
+        self.shapes = {"learned": sh_nms, "plain": sh_spa}
+        self.nms = g.LdpcDecoder(self.code, threads_per_block=sh_nms[0], blocks_per_sm=sh_nms[1], **kw_nms)
+        self.spa = g.LdpcDecoder(self.code, threads_per_block=sh_spa[0], blocks_per_sm=sh_spa[1], **kw_spa)
         self.out = None
         self.desc = (f"dvbt2-normal-2/3 learned normalised/offset min-sum ({self.T} layered iterations, per-iteration "
                      f"per-row-group weights {self.weights_desc}), fp16 messages, {self.frames} frames, "
                      f"frame f at Eb/N0 {pts[0]:.1f}+0.1*(f mod {len(pts)}) dB, early stop; frames still failing "
                      f"the syndrome re-decoded on the device by layered sum-product (SFU) max 50 it; compared with "
-                     f"layered sum-product (SFU) max 50 it alone on the same frames")
+                     f"layered sum-product (SFU) max 50 it alone on the same frames; autotuned launch shapes "
+                     f"(threads, CTAs/SM; 0 = default) learned {tuple(sh_nms)}, plain {tuple(sh_spa)}")
         self.dtype = "f16 storage / f32 math"
 
     def step(self):
@@ -492,6 +508,8 @@ class LearnedScale:
         return int(wrong.sum()), {f"{p:.1f}": int(x) for p, x in zip(C5_POINTS, per.tolist())}, n
 
     def stats(self):
+        import numpy as np
+
         from gf2_b200.montecarlo import wilson
         torch = self.torch
         it = self.out["iters"].cpu().numpy()
@@ -523,7 +541,8 @@ class LearnedScale:
                  "fer": fe_p / self.frames, "fer_ci": wilson(fe_p, self.frames), "frame_errors_per_ebn0": per_p}
         return b, {"mean": float(it.mean()), "max": int(it.max()),
                    "converged_frac": float(self.out["conv"].float().mean().item()),
-                   "fallback_frames": fb, "frame_iterations": int(it.sum()),
+                   "fallback_frames": fb, "frame_iterations": int(np.minimum(it, self.T).sum()),
+                   "frame_iterations_all_passes": int(it.sum()),
                    "fer": {"learned_with_fallback": fe / self.frames,
                            "learned_with_fallback_ci": wilson(fe, self.frames),
                            "frame_errors_per_ebn0": per, "frames_per_ebn0": n,

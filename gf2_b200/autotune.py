@@ -1,8 +1,9 @@
 """Launch-shape autotuner for the decoders.
 
 A decoder runs a persistent kernel in which each CTA decodes one frame at a
-time; its launch shape is (threads per block, CTAs per SM), i.e. the check /
-variable tile a thread steps over and the number of frames in flight per SM.
+time; its launch shape is (threads per block, CTAs per SM), i.e. the checks a
+thread steps over in each row group (the tile) and the number of frames in
+flight per SM.
 The autotuner times every feasible shape on a sample batch with CUDA events
 and keeps the fastest; results are cached in a JSON file keyed by device name,
 the build of the library (a hash of libgf2cuda.so), codes, algorithm, schedule
@@ -57,12 +58,18 @@ def _key(codes, algorithm, schedule, msg_dtype, device_name):
     return f"{device_name}|lib {library_hash()}|{cs}|a{algorithm}|s{schedule}|m{msg_dtype}"
 
 
-def candidates(codes, schedule):
-    """(threads per block, CTAs per SM) pairs; 0 = library choice.  The layered
-    schedule needs one thread per check of a row group, so only the number of
-    frames in flight per SM varies."""
+def candidates(codes, schedule, msg_dtype=0, algorithm=3):
+    """(threads per block, CTAs per SM) pairs; 0 = library choice.  Layered:
+    one thread per check of a row group (threads 0 = the row group rounded up
+    to 32), or for one code with FP16 messages and a fused-row algorithm 192 /
+    128 threads (each thread two / three checks, so four / six frames in
+    flight per SM at the same registers); the CTAs per SM vary within what
+    fits.  Shapes a decoder cannot have are skipped when it fails to build."""
     if schedule == 1:
-        return [(0, b) for b in (1, 2, 3, 4)]
+        c = [(0, b) for b in (0, 1)]
+        if len(codes) == 1 and msg_dtype == 1 and algorithm != 1:
+            c += [(192, b) for b in (0, 3)] + [(128, b) for b in (0, 4)]
+        return c
     return [(t, b) for t in (128, 256, 384, 512) for b in (0, 1, 2, 3, 4)]
 
 
@@ -78,7 +85,7 @@ def tune(codes, algorithm, schedule, msg_dtype, run, reps=3, nms_alpha=None, nms
         return (e["threads"], e["blocks_per_sm"]), e.get("table", [])
     table = []
     best = None
-    for threads, bps in candidates(codes, schedule):
+    for threads, bps in candidates(codes, schedule, msg_dtype, algorithm):
         try:
             dec = LdpcDecoder(codes[0], codes=codes, algorithm=algorithm, schedule=schedule, msg_dtype=msg_dtype,
                               nms_alpha=nms_alpha, nms_beta=nms_beta, threads_per_block=threads,

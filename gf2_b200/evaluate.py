@@ -106,7 +106,7 @@ def main(argv=None):
     p.add_argument("--decoders", default="learned,minsum,spa50")
     p.add_argument("--weights", default=None, help="load trained weights (npz) instead of training")
     p.add_argument("--save-weights", default=None)
-    p.add_argument("--throughput-ebn0", type=float, default=None)
+    p.add_argument("--throughput-ebn0", default=None, help="Eb/N0 (comma list) of the throughput measurements")
     p.add_argument("--out", default=None)
     a = p.parse_args(argv)
     dev = torch.device("cuda", 0)
@@ -159,10 +159,14 @@ def main(argv=None):
             curves[name].append(r)
             print(json.dumps(r), flush=True)
     cross = {k: crossing(v, a.target_fer) for k, v in curves.items()}
-    eb_tp = a.throughput_ebn0
-    if eb_tp is None:
-        eb_tp = cross.get("spa50") if cross.get("spa50") is not None else points[len(points) // 2]
-    tp = {k: throughput(d, code, eb_tp, iters[k], a.throughput_frames, dev) for k, d in decs.items()}
+    if a.throughput_ebn0 is None:
+        tp_points = [cross.get("spa50") if cross.get("spa50") is not None else points[len(points) // 2]]
+    else:
+        tp_points = [float(x) for x in a.throughput_ebn0.split(",")]
+    tp_all = {f"{e:.2f}": {k: throughput(d, code, e, iters[k], a.throughput_frames, dev) for k, d in decs.items()}
+              for e in tp_points}
+    eb_tp = tp_points[0]
+    tp = tp_all[f"{eb_tp:.2f}"]
 
     def diff(x, y):
         return (cross[x] - cross[y]) if cross.get(x) is not None and cross.get(y) is not None else None
@@ -174,7 +178,7 @@ def main(argv=None):
         gap_db_learned_vs_spa50=diff("learned", "spa50"),
         gap_db_learned_vs_spa50_layered=diff("learned", "spa50_layered"),
         gain_db_learned_vs_minsum=diff("minsum", "learned"),
-        throughput_at_ebn0=eb_tp, throughput=tp,
+        throughput_at_ebn0=eb_tp, throughput=tp, throughput_per_ebn0=tp_all,
         speedup_learned_vs_spa50=(tp["learned"]["gbit_s"] / tp["spa50"]["gbit_s"])
         if "learned" in tp and "spa50" in tp else None,
         alpha_mean_per_iter=[round(float(x), 4) for x in alpha.mean(axis=1)],

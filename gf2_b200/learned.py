@@ -209,6 +209,8 @@ class NmsTrainer:
         self.frame_counter = int(z["frames"])
         self.seed = int(z["seed"])
         self.history = list(z["history"])
+        if "ebn0" in z.files:
+            self.ebn0_range = (float(z["ebn0"][0]), float(z["ebn0"][1]))
         return self
 
 
