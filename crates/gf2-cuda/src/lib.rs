@@ -332,3 +332,79 @@ impl BlockEncoder for CudaLdpcEncoder<'_> {
         self.encode_batch(std::slice::from_ref(message)).pop().expect("one message in, one codeword out")
     }
 }
+
+/// DVB-T2 outer BCH code (`BchCode::dvb_t2`, crates/gf2-coding/src/bch/dvb_t2/mod.rs:62-78)
+/// with batch encode / decode (`BchEncoder::encode_batch`, `BchDecoder::decode_batch`,
+/// bch/core.rs:396-665): n of the BCH code is k of the matching LDPC code, so an
+/// LDPC decode's message bits are a BCH codeword.
+pub struct CudaBchCode {
+    raw: *mut ffi::gf2c_bch,
+    n: usize,
+    k: usize,
+}
+
+unsafe impl Send for CudaBchCode {}
+
+impl CudaBchCode {
+    pub fn dvb_t2(frame: i32, rate: DvbRate) -> Self {
+        let mut raw = ptr::null_mut();
+        check(unsafe { ffi::gf2c_bch_create_dvbt2(frame, rate as i32, &mut raw) });
+        let (mut n, mut k, mut t, mut m) = (0i64, 0i64, 0i32, 0i32);
+        check(unsafe { ffi::gf2c_bch_dims(raw, &mut n, &mut k, &mut t, &mut m) });
+        Self { raw, n: n as usize, k: k as usize }
+    }
+
+    pub fn n(&self) -> usize {
+        self.n
+    }
+    pub fn k(&self) -> usize {
+        self.k
+    }
+
+    /// Systematic codewords [message | parity] of a batch of messages.
+    pub fn encode_batch(&mut self, messages: &[BitVec]) -> Vec<BitVec> {
+        let (wk, wn, f) = (words(self.k), words(self.n), messages.len());
+        if f == 0 {
+            return Vec::new();
+        }
+        let mut msg = Vec::with_capacity(f * wk);
+        for m in messages {
+            assert_eq!(m.len(), self.k, "message length must equal k");
+            msg.extend_from_slice(m.words());
+        }
+        let mut cw = vec![0u64; f * wn];
+        check(unsafe {
+            ffi::gf2c_bch_encode_batch(self.raw, msg.as_ptr(), f as i64, cw.as_mut_ptr(), ffi::GF2C_MEM_HOST,
+                                       ptr::null_mut())
+        });
+        cw.chunks(wn).map(|w| BitVec::from_words(w.to_vec(), self.n)).collect()
+    }
+
+    /// Hard-decision decode of a batch of received words (bit-identical to
+    /// `BchDecoder::decode`, including its behaviour beyond t errors).
+    pub fn decode_batch(&mut self, received: &[BitVec]) -> Vec<BitVec> {
+        let (wk, wn, f) = (words(self.k), words(self.n), received.len());
+        if f == 0 {
+            return Vec::new();
+        }
+        let mut cw = Vec::with_capacity(f * wn);
+        for r in received {
+            assert_eq!(r.len(), self.n, "received word length must equal n");
+            cw.extend_from_slice(r.words());
+        }
+        let mut msg = vec![0u64; f * wk];
+        check(unsafe {
+            ffi::gf2c_bch_decode_batch(self.raw, cw.as_ptr(), f as i64, msg.as_mut_ptr(), ptr::null_mut(),
+                                       ptr::null_mut(), ffi::GF2C_MEM_HOST, ptr::null_mut())
+        });
+        msg.chunks(wk).map(|w| BitVec::from_words(w.to_vec(), self.k)).collect()
+    }
+}
+
+impl Drop for CudaBchCode {
+    fn drop(&mut self) {
+        unsafe {
+            ffi::gf2c_bch_destroy(self.raw);
+        }
+    }
+}
