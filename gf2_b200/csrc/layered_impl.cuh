@@ -457,199 +457,6 @@ __device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int
   }
 }
 
-// Two checks ta, tb of a row group without repeated variables, decoded
-// together by one thread (several checks per thread, staged old messages):
-// the posterior loads of both checks are issued before either check's stores,
-// so their latencies overlap.  The arithmetic of each check is that of ms_row
-// / spa_fast_row (old messages re-read from the stage instead of kept in
-// registers; the SFU path recomputes e = 2^(-|x| log2 e) in its second pass,
-// the same operation), so results are bit-identical.
-template <int MSG16>
-__device__ __forceinline__ float lds_msg(uint32_t a) {
-  if constexpr (MSG16) {
-    unsigned short h;
-    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(h) : "r"(a));
-    return __half2float(__ushort_as_half(h));
-  } else {
-    float x;
-    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(x) : "r"(a));
-    return x;
-  }
-}
-
-template <int ALGO, int MSG16, int D, bool PART>
-__device__ __forceinline__ void ms_row_pair(const int2* __restrict__ sd, int ta, int tb, int nchk, int edge0,
-                                            float* app, typename MsgIO<MSG16>::T* __restrict__ c2v, uint32_t oa,
-                                            uint32_t ob, uint32_t stride, bool first, float al, float be,
-                                            const LayerSmem& S, const int2* __restrict__ vg,
-                                            const int* __restrict__ ci, int vgs, int d) {
-  typedef MsgIO<MSG16> IO;
-  float pa[D], pb[D];
-#pragma unroll
-  for (int i = 0; i < D; i++) {
-    if (PART && i >= d) continue;
-    const int2 Dd = __ldg(&sd[i]);
-    pa[i] = app[slot_u(Dd, ta, nchk)];
-    pb[i] = app[slot_u(Dd, tb, nchk)];
-  }
-  float m1a = __int_as_float(0x7f800000), m2a = m1a, m1b = m1a, m2b = m1a;
-  int i1a = -1, i1b = -1;
-  uint32_t nega = 0, negb = 0, apa = 0, apb = 0;
-#pragma unroll
-  for (int i = 0; i < D; i++) {
-    if (PART && i >= d) continue;
-    const float oA = first ? 0.0f : lds_msg<MSG16>(oa + i * stride);
-    const float oB = first ? 0.0f : lds_msg<MSG16>(ob + i * stride);
-    const float wa = __fsub_rn(pa[i], oA), wb = __fsub_rn(pb[i], oB);
-    const float xa = fabsf(wa), xb = fabsf(wb);
-    if (xa < m1a) {
-      m2a = m1a;
-      m1a = xa;
-      i1a = i;
-    } else if (xa < m2a) {
-      m2a = xa;
-    }
-    if (xb < m1b) {
-      m2b = m1b;
-      m1b = xb;
-      i1b = i;
-    } else if (xb < m2b) {
-      m2b = xb;
-    }
-    nega |= (uint32_t)(wa < 0.0f) << i;
-    negb |= (uint32_t)(wb < 0.0f) << i;
-    apa |= (uint32_t)(pa[i] < 0.0f) << i;
-    apb |= (uint32_t)(pb[i] < 0.0f) << i;
-  }
-  float ma1 = m1a, ma2 = m2a, mb1 = m1b, mb2 = m2b;
-  if (ALGO == L_NMS) {
-    float t1 = __fsub_rn(ma1, be), t2 = __fsub_rn(ma2, be);
-    ma1 = __fmul_rn(al, t1 > 0.0f ? t1 : 0.0f);
-    ma2 = __fmul_rn(al, t2 > 0.0f ? t2 : 0.0f);
-    t1 = __fsub_rn(mb1, be);
-    t2 = __fsub_rn(mb2, be);
-    mb1 = __fmul_rn(al, t1 > 0.0f ? t1 : 0.0f);
-    mb2 = __fmul_rn(al, t2 > 0.0f ? t2 : 0.0f);
-  }
-  const uint32_t npa = __popc(nega) & 1u, npb = __popc(negb) & 1u;
-  uint32_t fa = 0, fb = 0;
-#pragma unroll
-  for (int i = 0; i < D; i++) {
-    if (PART && i >= d) continue;
-    const int2 Dd = __ldg(&sd[i]);
-    const float oA = first ? 0.0f : lds_msg<MSG16>(oa + i * stride);
-    const float outa = IO::rt((npa ^ ((nega >> i) & 1u)) ? -((i == i1a) ? ma2 : ma1) : ((i == i1a) ? ma2 : ma1));
-    st_msg<MSG16>(c2v, edge0 + ta + i * nchk, outa);
-    const float nwa = __fadd_rn(pa[i], __fsub_rn(outa, oA));
-    app[slot_u(Dd, ta, nchk)] = nwa;
-    fa |= (uint32_t)(((apa >> i) & 1u) != (uint32_t)(nwa < 0.0f)) << i;
-    const float oB = first ? 0.0f : lds_msg<MSG16>(ob + i * stride);
-    const float outb = IO::rt((npb ^ ((negb >> i) & 1u)) ? -((i == i1b) ? mb2 : mb1) : ((i == i1b) ? mb2 : mb1));
-    st_msg<MSG16>(c2v, edge0 + tb + i * nchk, outb);
-    const float nwb = __fadd_rn(pb[i], __fsub_rn(outb, oB));
-    app[slot_u(Dd, tb, nchk)] = nwb;
-    fb |= (uint32_t)(((apb >> i) & 1u) != (uint32_t)(nwb < 0.0f)) << i;
-  }
-  while (fa) {
-    const int i = __ffs(fa) - 1;
-    fa &= fa - 1;
-    flip_var(slot_u(__ldg(&sd[i]), ta, nchk), S, vg, ci, vgs);
-  }
-  while (fb) {
-    const int i = __ffs(fb) - 1;
-    fb &= fb - 1;
-    flip_var(slot_u(__ldg(&sd[i]), tb, nchk), S, vg, ci, vgs);
-  }
-}
-
-template <int MSG16, int D, bool PART>
-__device__ __forceinline__ void spa_fast_row_pair(const int2* __restrict__ sd, int ta, int tb, int nchk, int edge0,
-                                                  float* app, typename MsgIO<MSG16>::T* __restrict__ c2v, uint32_t oa,
-                                                  uint32_t ob, uint32_t stride, bool first, const LayerSmem& S,
-                                                  const int2* __restrict__ vg, const int* __restrict__ ci, int vgs,
-                                                  int d) {
-  typedef MsgIO<MSG16> IO;
-  float xa[D], xb[D];
-#pragma unroll
-  for (int i = 0; i < D; i++) {
-    if (!PART || i < d) {
-      const int2 Dd = __ldg(&sd[i]);
-      xa[i] = app[slot_u(Dd, ta, nchk)];
-      xb[i] = app[slot_u(Dd, tb, nchk)];
-    } else {
-      xa[i] = 3.402823466e38f;
-      xb[i] = 3.402823466e38f;
-    }
-  }
-  uint32_t nega = 0, negb = 0, apa = 0, apb = 0;
-#pragma unroll
-  for (int i = 0; i < D; i++) {
-    apa |= (uint32_t)(xa[i] < 0.0f) << i;
-    apb |= (uint32_t)(xb[i] < 0.0f) << i;
-  }
-  if (!first) {
-#pragma unroll
-    for (int i = 0; i < D; i++)
-      if (!PART || i < d) {
-        xa[i] = __fsub_rn(xa[i], lds_msg<MSG16>(oa + i * stride));
-        xb[i] = __fsub_rn(xb[i], lds_msg<MSG16>(ob + i * stride));
-      }
-  }
-  float Na = 1.0f, Da = 1.0f, Nb = 1.0f, Db = 1.0f;
-#pragma unroll
-  for (int i = 0; i < D; i++) {
-    nega |= (uint32_t)(xa[i] < 0.0f) << i;
-    negb |= (uint32_t)(xb[i] < 0.0f) << i;
-    const float ea = ex2_approx(fabsf(xa[i]) * -1.4426950408889634f);
-    const float eb = ex2_approx(fabsf(xb[i]) * -1.4426950408889634f);
-    Na *= fmaxf(1.0f - ea, 5.9604645e-08f);
-    Da = __fmaf_rn(Da, ea, Da);
-    Nb *= fmaxf(1.0f - eb, 5.9604645e-08f);
-    Db = __fmaf_rn(Db, eb, Db);
-  }
-  const uint32_t npa = __popc(nega) & 1u, npb = __popc(negb) & 1u;
-  uint32_t fa = 0, fb = 0;
-#pragma unroll
-  for (int i = 0; i < D; i++) {
-    if (PART && i >= d) continue;
-    const int2 Dd = __ldg(&sd[i]);
-    {
-      const float e = ex2_approx(fabsf(xa[i]) * -1.4426950408889634f);
-      const float ni = fmaxf(1.0f - e, 5.9604645e-08f), di = 1.0f + e;
-      const float num = __fmaf_rn(Da, ni, Na * di);
-      const float den = fmaxf(__fmaf_rn(Da, ni, -Na * di), num * 5.9604645e-08f);
-      const float mag = fminf(0.69314718055994531f * lg2_approx(num * rcp_approx(den)), 16.635532f);
-      const float out = IO::rt((npa ^ ((nega >> i) & 1u)) ? -mag : mag);
-      st_msg<MSG16>(c2v, edge0 + ta + i * nchk, out);
-      const float nw = xa[i] + out;
-      app[slot_u(Dd, ta, nchk)] = nw;
-      fa |= (uint32_t)(((apa >> i) & 1u) != (uint32_t)(nw < 0.0f)) << i;
-    }
-    {
-      const float e = ex2_approx(fabsf(xb[i]) * -1.4426950408889634f);
-      const float ni = fmaxf(1.0f - e, 5.9604645e-08f), di = 1.0f + e;
-      const float num = __fmaf_rn(Db, ni, Nb * di);
-      const float den = fmaxf(__fmaf_rn(Db, ni, -Nb * di), num * 5.9604645e-08f);
-      const float mag = fminf(0.69314718055994531f * lg2_approx(num * rcp_approx(den)), 16.635532f);
-      const float out = IO::rt((npb ^ ((negb >> i) & 1u)) ? -mag : mag);
-      st_msg<MSG16>(c2v, edge0 + tb + i * nchk, out);
-      const float nw = xb[i] + out;
-      app[slot_u(Dd, tb, nchk)] = nw;
-      fb |= (uint32_t)(((apb >> i) & 1u) != (uint32_t)(nw < 0.0f)) << i;
-    }
-  }
-  while (fa) {
-    const int i = __ffs(fa) - 1;
-    fa &= fa - 1;
-    flip_var(slot_u(__ldg(&sd[i]), ta, nchk), S, vg, ci, vgs);
-  }
-  while (fb) {
-    const int i = __ffs(fb) - 1;
-    fb &= fb - 1;
-    flip_var(slot_u(__ldg(&sd[i]), tb, nchk), S, vg, ci, vgs);
-  }
-}
-
 // General check update (any algorithm, absent slots, repeated variables):
 // 1. indices, 2. all loads, 3. arithmetic, 4. message stores.  With
 // `direct` (a row group without repeated variables) the posteriors are
@@ -881,31 +688,7 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
         __syncthreads();
         for (int tc = tid; tc < nchk; tc += NT) spa_fast_rep_b<DCMAX>(sd, tc, nchk, app, sync, S.dbuf, S, vg, vg_chk, vgs);
       } else if (sync == 0) {
-        int tc0 = tid;
-        if constexpr (STG && kFused && MULTI) {
-          // several checks per thread: two checks at a time where the thread has two
-          for (; tc0 + NT < nchk; tc0 += 2 * NT) {
-            const uint32_t ab = (tc0 == 0) ? __ldg(&absent[g]) : 0u;
-            if (!(d >= 2 && d <= DCMAX && ab == 0)) break;  // this pair takes the single path below
-            const uint32_t oa = old_of(tc0).a, ob = old_of(tc0 + NT).a;
-            if constexpr (ALGO == L_SPA_FAST) {
-              if (d == DCMAX)
-                spa_fast_row_pair<MSG16, DCMAX, false>(sd, tc0, tc0 + NT, nchk, G.w, app, c2v, oa, ob, om.stride,
-                                                       first, S, vg, vg_chk, vgs, d);
-              else
-                spa_fast_row_pair<MSG16, DCMAX, true>(sd, tc0, tc0 + NT, nchk, G.w, app, c2v, oa, ob, om.stride,
-                                                      first, S, vg, vg_chk, vgs, d);
-            } else {
-              if (d == DCMAX)
-                ms_row_pair<ALGO, MSG16, DCMAX, false>(sd, tc0, tc0 + NT, nchk, G.w, app, c2v, oa, ob, om.stride,
-                                                       first, al, be, S, vg, vg_chk, vgs, d);
-              else
-                ms_row_pair<ALGO, MSG16, DCMAX, true>(sd, tc0, tc0 + NT, nchk, G.w, app, c2v, oa, ob, om.stride,
-                                                      first, al, be, S, vg, vg_chk, vgs, d);
-            }
-          }
-        }
-        for (int tc = tc0; tc < nchk; tc += NT) {
+        for (int tc = tid; tc < nchk; tc += NT) {
           const OM omc = old_of(tc);
           const int sc = G.w + tc;
           const uint32_t ab = (tc == 0) ? __ldg(&absent[g]) : 0u;
