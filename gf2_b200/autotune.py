@@ -63,12 +63,12 @@ def candidates(codes, schedule, msg_dtype=0, algorithm=3):
     one thread per check of a row group (threads 0 = the row group rounded up
     to 32), or for one code with FP16 messages and a fused-row algorithm 192 /
     128 threads (each thread two / three checks, so four / six frames in
-    flight per SM at the same registers); the CTAs per SM vary within what
-    fits.  Shapes a decoder cannot have are skipped when it fails to build."""
+    flight per SM at the same registers; 192 threads with 5 CTAs per SM is a
+    64-register build); the CTAs per SM vary within what fits.  Shapes a decoder cannot have are skipped when it fails to build."""
     if schedule == 1:
         c = [(0, b) for b in (0, 1)]
         if len(codes) == 1 and msg_dtype == 1 and algorithm != 1:
-            c += [(192, b) for b in (0, 3)] + [(128, b) for b in (0, 4)]
+            c += [(192, b) for b in (0, 3, 5)] + [(128, b) for b in (0, 4)]
         return c
     return [(t, b) for t in (128, 256, 384, 512) for b in (0, 1, 2, 3, 4)]
 

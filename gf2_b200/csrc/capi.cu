@@ -495,7 +495,8 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
       ok = ok && off % 16 == 0 && by % 16 == 0;
       mx = std::max(mx, by);
     }
-    const void* k = ok ? layered_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax, threads, true) : nullptr;
+    const void* k = ok ? layered_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax, threads, true, o.blocks_per_sm)
+                       : nullptr;
     int optin = 0, occ0 = 0, occ1 = 0;
     GF2C_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->dev));
     const size_t off = (d->smem + 15) & ~(size_t)15, with = off + 2 * mx + 16;

@@ -225,7 +225,8 @@ int state_flood_threads();
 const void* state_flood_kernel_ptr(int dcmax, bool all_smem);
 int decode_dcmax_bucket(int max_dc);
 int layered_dcmax_bucket(int max_dc);
-const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt, bool stage = false);
+// bps: requested CTAs per SM (0 = any); 192 threads with 5 or more picks the 64-register build
+const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt, bool stage = false, int bps = 0);
 size_t layered_smem_bytes(int smem_app_floats, int bitmap_words, int parity_words);
 size_t decode_smem_bytes(int smem_app_floats, int bitmap_words);
 

@@ -3,6 +3,6 @@
 
 namespace gf2c {
 
-const void* layered_spa16_kernel(int dcmax, int maxt, bool stage) { return lay_t<L_SPA, 1>(dcmax, maxt, stage); }
+const void* layered_spa16_kernel(int dcmax, int maxt, bool stage, int bps) { return lay_t<L_SPA, 1>(dcmax, maxt, stage, bps); }
 
 }  // namespace gf2c

@@ -443,10 +443,11 @@ def test_edge_cases(gpu, oracle):
 
 @pytest.mark.parametrize("idx,algo", [(1, g.ALGO_SPA_FAST), (1, g.ALGO_NMS), (2, g.ALGO_MINSUM), (6, g.ALGO_SPA_FAST),
                                       (5, g.ALGO_NMS), (9, g.ALGO_SPA_FAST)])
-@pytest.mark.parametrize("threads", [192, 128])
-def test_layered_shapes_bit_identical(gpu, oracle, idx, algo, threads):
+@pytest.mark.parametrize("threads,bps", [(192, 0), (192, 5), (128, 0)])
+def test_layered_shapes_bit_identical(gpu, oracle, idx, algo, threads, bps):
     """Several checks per thread (192 / 128 threads, more frames in flight per
-    SM) give results bit-identical to one thread per check, for codes with
+    SM; 192 threads at 5 CTAs per SM is a separate 64-register build) give
+    results bit-identical to one thread per check, for codes with
     repeated-variable row groups (normal 3/5, 5/6), the missing staircase
     corner, and short frames (posteriors in shared memory)."""
     import torch
@@ -461,7 +462,7 @@ def test_layered_shapes_bit_identical(gpu, oracle, idx, algo, threads):
     _, _, llr = g.awgn_frames(code, 17, 0, 400, g.sigma2_from_ebn0(ebn0, code.rate()), device=gpu,
                               want_info=False, want_cw=False)
     ref = g.LdpcDecoder(code, **kw).decode_tensors(llr, 30, beliefs=True)
-    r = g.LdpcDecoder(code, threads_per_block=threads, **kw).decode_tensors(llr, 30, beliefs=True)
+    r = g.LdpcDecoder(code, threads_per_block=threads, blocks_per_sm=bps, **kw).decode_tensors(llr, 30, beliefs=True)
     torch.cuda.synchronize()
     for key in ("msg", "iters", "conv", "synd_ok"):
         assert torch.equal(r[key], ref[key]), key
