@@ -89,14 +89,12 @@ __device__ __forceinline__ void st_msg<1>(__half* p, int s, float v) {
 // message array, or at a shared-memory stage that a TMA copy filled.
 template <int MSG16>
 struct GlobalOld {
-  static constexpr bool kShared = false;
   const typename MsgIO<MSG16>::T* p;  // c2v + edge0 + t
   int nchk;
   __device__ __forceinline__ float ld(int i) const { return ld_msg<MSG16>(p, i * nchk); }
 };
 template <int MSG16>
 struct SharedOld {
-  static constexpr bool kShared = true;
   uint32_t a;       // shared address of slot 0 of the check
   uint32_t stride;  // bytes between slots (nchk messages)
   __device__ __forceinline__ float ld(int i) const {
@@ -215,10 +213,7 @@ __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t,
                                              const LayerSmem& S, const int2* __restrict__ vg,
                                              const int* __restrict__ ci, int vgs, int d) {
   typedef MsgIO<MSG16> IO;
-  // staged kernels recompute e in the second pass (the same operation) instead
-  // of keeping it live
-  constexpr bool kReload = OM::kShared;
-  float x[D], e[kReload ? 1 : D];
+  float x[D], e[D];
 #pragma unroll
   for (int i = 0; i < D; i++) x[i] = (!PART || i < d) ? app[slot_u(__ldg(&sd[i]), t, nchk)] : 3.402823466e38f;
   uint32_t neg = 0, apneg = 0;
@@ -233,21 +228,15 @@ __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t,
 #pragma unroll
   for (int i = 0; i < D; i++) {
     neg |= (uint32_t)(x[i] < 0.0f) << i;
-    const float ei = ex2_approx(fabsf(x[i]) * -1.4426950408889634f);
-    if constexpr (!kReload) e[i] = ei;
-    N *= fmaxf(1.0f - ei, 5.9604645e-08f);
-    Dp = __fmaf_rn(Dp, ei, Dp);
+    e[i] = ex2_approx(fabsf(x[i]) * -1.4426950408889634f);
+    N *= fmaxf(1.0f - e[i], 5.9604645e-08f);
+    Dp = __fmaf_rn(Dp, e[i], Dp);
   }
   const uint32_t negp = __popc(neg) & 1u;
   uint32_t flips = 0;
 #pragma unroll
   for (int i = 0; i < D; i++) {
-    float ei;
-    if constexpr (kReload)
-      ei = ex2_approx(fabsf(x[i]) * -1.4426950408889634f);
-    else
-      ei = e[i];
-    const float ni = fmaxf(1.0f - ei, 5.9604645e-08f), di = 1.0f + ei;
+    const float ni = fmaxf(1.0f - e[i], 5.9604645e-08f), di = 1.0f + e[i];
     const float num = __fmaf_rn(Dp, ni, N * di);
     const float den = fmaxf(__fmaf_rn(Dp, ni, -N * di), num * 5.9604645e-08f);
     const float mag = fminf(0.69314718055994531f * lg2_approx(num * rcp_approx(den)), 16.635532f);
@@ -283,8 +272,7 @@ __device__ __forceinline__ void spa_fast_rep_a(const int2* __restrict__ sd, int 
                                                int d) {
   typedef MsgIO<MSG16> IO;
   const uint32_t rep = sync | (sync << 1);  // slots inside a run
-  constexpr bool kReload = OM::kShared;     // recompute e in the second pass (see spa_fast_row)
-  float x[D], e[kReload ? 1 : D];
+  float x[D], e[D];
 #pragma unroll
   for (int i = 0; i < D; i++) x[i] = (!PART || i < d) ? app[slot_u(__ldg(&sd[i]), t, nchk)] : 3.402823466e38f;
 #pragma unroll
@@ -300,20 +288,14 @@ __device__ __forceinline__ void spa_fast_rep_a(const int2* __restrict__ sd, int 
 #pragma unroll
   for (int i = 0; i < D; i++) {
     neg |= (uint32_t)(x[i] < 0.0f) << i;
-    const float ei = ex2_approx(fabsf(x[i]) * -1.4426950408889634f);
-    if constexpr (!kReload) e[i] = ei;
-    N *= fmaxf(1.0f - ei, 5.9604645e-08f);
-    Dp = __fmaf_rn(Dp, ei, Dp);
+    e[i] = ex2_approx(fabsf(x[i]) * -1.4426950408889634f);
+    N *= fmaxf(1.0f - e[i], 5.9604645e-08f);
+    Dp = __fmaf_rn(Dp, e[i], Dp);
   }
   const uint32_t negp = __popc(neg) & 1u;
 #pragma unroll
   for (int i = 0; i < D; i++) {
-    float ei;
-    if constexpr (kReload)
-      ei = ex2_approx(fabsf(x[i]) * -1.4426950408889634f);
-    else
-      ei = e[i];
-    const float ni = fmaxf(1.0f - ei, 5.9604645e-08f), di = 1.0f + ei;
+    const float ni = fmaxf(1.0f - e[i], 5.9604645e-08f), di = 1.0f + e[i];
     const float num = __fmaf_rn(Dp, ni, N * di);
     const float den = fmaxf(__fmaf_rn(Dp, ni, -N * di), num * 5.9604645e-08f);
     const float mag = fminf(0.69314718055994531f * lg2_approx(num * rcp_approx(den)), 16.635532f);
@@ -368,29 +350,18 @@ __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int n
                                        const LayerSmem& S, const int2* __restrict__ vg, const int* __restrict__ ci,
                                        int vgs, int d) {
   typedef MsgIO<MSG16> IO;
-  // staged old messages are re-read from shared memory where they are needed
-  // again (fewer live registers); streamed ones are kept
-  constexpr bool kReload = OM::kShared;
-  float ap[D], o[kReload ? 1 : D];
+  float ap[D], o[D];
 #pragma unroll
   for (int i = 0; i < D; i++) ap[i] = (!PART || i < d) ? app[slot_u(__ldg(&sd[i]), t, nchk)] : 0.0f;
-  if constexpr (!kReload) {
 #pragma unroll
-    for (int i = 0; i < D; i++) o[i] = (first || (PART && i >= d)) ? 0.0f : om.ld(i);
-  }
-  auto old_msg = [&](int i) -> float {
-    if constexpr (kReload)
-      return first ? 0.0f : om.ld(i);
-    else
-      return o[i];
-  };
+  for (int i = 0; i < D; i++) o[i] = (first || (PART && i >= d)) ? 0.0f : om.ld(i);
   float m1 = __int_as_float(0x7f800000), m2 = m1;
   int i1 = -1;
   uint32_t neg = 0, apneg = 0;
 #pragma unroll
   for (int i = 0; i < D; i++) {
     if (PART && i >= d) continue;
-    const float w = __fsub_rn(ap[i], old_msg(i));
+    const float w = __fsub_rn(ap[i], o[i]);
     const float ax = fabsf(w);
     if (ax < m1) {
       m2 = m1;
@@ -416,7 +387,7 @@ __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int n
     const float mag = (i == i1) ? mag2 : mag1;
     const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
     st_msg<MSG16>(c2v, s0 + i * nchk, out);
-    const float nw = __fadd_rn(ap[i], __fsub_rn(out, old_msg(i)));
+    const float nw = __fadd_rn(ap[i], __fsub_rn(out, o[i]));
     app[slot_u(__ldg(&sd[i]), t, nchk)] = nw;
     flips |= (uint32_t)(((apneg >> i) & 1u) != (uint32_t)(nw < 0.0f)) << i;
   }
@@ -441,29 +412,18 @@ __device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int
                                          const int2* __restrict__ vg, const int* __restrict__ ci, int vgs, int d) {
   typedef MsgIO<MSG16> IO;
   const uint32_t rep = sync | (sync << 1);  // slots inside a run
-  // staged old messages are re-read from shared memory where they are needed
-  // again (fewer live registers); streamed ones are kept
-  constexpr bool kReload = OM::kShared;
-  float ap[D], o[kReload ? 1 : D];
+  float ap[D], o[D];
 #pragma unroll
   for (int i = 0; i < D; i++) ap[i] = (!PART || i < d) ? app[slot_u(__ldg(&sd[i]), t, nchk)] : 0.0f;
-  if constexpr (!kReload) {
 #pragma unroll
-    for (int i = 0; i < D; i++) o[i] = (first || (PART && i >= d)) ? 0.0f : om.ld(i);
-  }
-  auto old_msg = [&](int i) -> float {
-    if constexpr (kReload)
-      return first ? 0.0f : om.ld(i);
-    else
-      return o[i];
-  };
+  for (int i = 0; i < D; i++) o[i] = (first || (PART && i >= d)) ? 0.0f : om.ld(i);
   float m1 = __int_as_float(0x7f800000), m2 = m1;
   int i1 = -1;
   uint32_t neg = 0;
 #pragma unroll
   for (int i = 0; i < D; i++) {
     if (PART && i >= d) continue;
-    const float w = __fsub_rn(ap[i], old_msg(i));
+    const float w = __fsub_rn(ap[i], o[i]);
     const float ax = fabsf(w);
     if (ax < m1) {
       m2 = m1;
@@ -487,7 +447,7 @@ __device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int
     const float mag = (i == i1) ? mag2 : mag1;
     const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
     st_msg<MSG16>(c2v, s0 + i * nchk, out);
-    const float delta = __fsub_rn(out, old_msg(i));
+    const float delta = __fsub_rn(out, o[i]);
     if ((rep >> i) & 1u) {
       dbuf[i * nchk + t] = delta;
     } else {
