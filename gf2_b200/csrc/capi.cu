@@ -60,7 +60,7 @@ struct gf2c_decoder {
   int dev = 0;
   DevBuf d_codes;
   int max_n = 0, max_m = 0, max_words_k = 0, max_e_slots = 0, max_dc = 0, max_nchk = 0;
-  int dcmax = 0, threads = 0, grid = 0, bitmap_words = 0, parity_words = 0, smem_app_floats = 0;
+  int dcmax = 0, threads = 0, grid = 0, bitmap_words = 0, smem_app_floats = 0;
   int lay_dbuf_off = 0, lay_dbuf_floats = 0;
   int lay_stage_off = 0, lay_stage_bytes = 0;
   const void* kernel = nullptr;
@@ -388,9 +388,8 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   threads = std::max(threads, 32);
   d->threads = threads;
   d->bitmap_words = (d->max_n + 31) / 32;
-  d->parity_words = layered ? (d->max_m + 31) / 32 : 0;
   auto smem_of = [&](int app_floats) {
-    return layered ? layered_smem_bytes(app_floats, d->bitmap_words, d->parity_words)
+    return layered ? layered_smem_bytes(app_floats, d->bitmap_words)
                    : decode_smem_bytes(app_floats, d->bitmap_words);
   };
   // keep the APP of every code whose n fits in shared memory there
@@ -558,7 +557,6 @@ static int launch_decoder(gf2c_decoder* d, DecodeArgs& a, int64_t frames, cudaSt
   a.app_offset = d->app_offset;
   a.smem_app_floats = d->smem_app_floats;
   a.bitmap_words = d->bitmap_words;
-  a.parity_words = d->parity_words;
   a.lay_dbuf_off = d->lay_dbuf_off;
   a.lay_dbuf_floats = d->lay_dbuf_floats;
   a.lay_stage_off = d->lay_stage_off;

@@ -189,7 +189,6 @@ struct DecodeArgs {
   long long app_offset;            // offset of the global APP inside a CTA workspace
   int smem_app_floats;             // APP kept in shared memory when n <= this
   int bitmap_words;                // 32-bit words of the hard-decision bitmap
-  int parity_words;                // 32-bit words of the check-parity bitmap (layered)
   int lay_dbuf_off, lay_dbuf_floats;  // layered fused rows: shared-memory buffer of slots x checks
   int lay_stage_off, lay_stage_bytes; // layered, TMA-staged messages: two buffers of one row group's
                                       // messages, then two mbarriers (byte offset in dynamic smem)
@@ -227,7 +226,7 @@ int decode_dcmax_bucket(int max_dc);
 int layered_dcmax_bucket(int max_dc);
 // bps: requested CTAs per SM (0 = any); 192 threads with 5 or more picks the 64-register build
 const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt, bool stage = false, int bps = 0);
-size_t layered_smem_bytes(int smem_app_floats, int bitmap_words, int parity_words);
+size_t layered_smem_bytes(int smem_app_floats, int bitmap_words);
 size_t decode_smem_bytes(int smem_app_floats, int bitmap_words);
 
 int launch_nms_forward(const DevCode* dcode, const DevCode& h, int T, int L, const float* llr, const uint64_t* cw,

@@ -38,8 +38,8 @@ const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt, bool st
   return nullptr;
 }
 
-size_t layered_smem_bytes(int smem_app_floats, int bitmap_words, int parity_words) {
-  return (size_t)(((bitmap_words + parity_words) * 4 + 15) & ~15) + (size_t)smem_app_floats * 4;
+size_t layered_smem_bytes(int smem_app_floats, int bitmap_words) {
+  return (size_t)((bitmap_words * 4 + 15) & ~15) + (size_t)smem_app_floats * 4;
 }
 
 }  // namespace gf2c

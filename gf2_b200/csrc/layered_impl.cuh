@@ -27,11 +27,14 @@
 // deltas slot by slot with a barrier between slots of the same block, i.e. in
 // ascending circulant shift.
 //
-// Early stop: instead of a syndrome pass per iteration, the kernel keeps the
-// parity of every check of the current hard decisions in shared memory and
-// the number of unsatisfied checks; a variable whose hard decision flips
-// toggles the parity of its checks.  The count is exact, so "count == 0 at
-// the end of an iteration" is the reference's syndrome test (core.rs:918-922).
+// Early stop: the hard decisions live in a shared-memory bitmap that a
+// posterior update toggles when its sign flips (one shared atomic, rare after
+// the first iterations); at the end of an iteration a syndrome pass over the
+// bitmap, row group by row group, stops at the first unsatisfied check.  That
+// is the reference's syndrome test (core.rs:918-922) at the cost of one row
+// group's bit gathers while a frame is far from a codeword.  (Keeping every
+// check's parity up to date on each flip instead, which needs the flipped
+// variable's check list from global memory, cost 30 % of the min-sum kernel.)
 //
 // Check-node rules: min-sum / normalised-offset min-sum / sum-product with the
 // exact library numerics (bit-identical to the CPU restatement), and a fast
@@ -165,8 +168,6 @@ struct Stage {
 
 struct LayerSmem {
   uint32_t* bitmap;   // hard decisions, n bits
-  uint32_t* chkpar;   // parity of each (flattened) check, m bits
-  int* unsat;         // number of unsatisfied checks
   float* dbuf;        // slots x checks of a row group: old messages / deltas (nullptr: none)
 };
 
@@ -175,29 +176,44 @@ struct LayerSmem {
 // t = 0 is masked separately).
 __device__ __forceinline__ int slot_u(const int2 D, int t, int Z) { return D.x + t - (t >= D.y ? Z : 0); }
 
-// A hard decision flipped: toggle it and the parity of the variable's checks
-// (u-order edge lists, flattened check | slot << 24), and update the number of
-// unsatisfied checks (rare after the first iterations).
-static __device__ __noinline__ void flip_var(int u, const LayerSmem S, const int2* __restrict__ vg,
-                                      const int* __restrict__ ci, int vgs) {
-  atomicXor(&S.bitmap[u >> 5], 1u << (u & 31));
-  const int h = u / vgs, j = u - h * vgs;
-  const int2 V = vg[h];
-  int delta = 0;
-  for (int i = 0; i < V.x; i++) {
-    const int e = __ldg(&ci[V.y + i * vgs + j]);
-    if (e < 0) break;
-    const int cc = e & 0xffffff;
-    const uint32_t was = atomicXor(&S.chkpar[cc >> 5], 1u << (cc & 31));
-    delta += ((was >> (cc & 31)) & 1u) ? -1 : 1;
-  }
-  atomicAdd(S.unsat, delta);
+// A hard decision flipped: toggle its bit (the bitmap is the syndrome pass's
+// input at the end of the iteration).
+__device__ __forceinline__ void flip_var(int u, const LayerSmem& S) { atomicXor(&S.bitmap[u >> 5], 1u << (u & 31)); }
+
+__device__ __forceinline__ void app_put(float* app, int v, bool old_neg, float nw, const LayerSmem& S) {
+  app[v] = nw;
+  if (old_neg != (nw < 0.0f)) flip_var(v, S);
 }
 
-__device__ __forceinline__ void app_put(float* app, int v, bool old_neg, float nw, const LayerSmem& S,
-                                        const int2* __restrict__ vg, const int* __restrict__ vg_chk, int vgs) {
-  app[v] = nw;
-  if (old_neg != (nw < 0.0f)) flip_var(v, S, vg, vg_chk, vgs);
+// Syndrome of the hard decisions in the bitmap: true when every check is
+// satisfied (the reference's test, core.rs:918-922).  Row groups in order, the
+// CTA's threads over the checks of a row group, one barrier per row group; the
+// pass stops at the first row group with an unsatisfied check, so a frame that
+// is still far from a codeword pays one row group.  Every thread returns after
+// the same barrier.
+template <int DCMAX>
+__device__ __forceinline__ bool syndrome_zero(const DevCode& C, const uint32_t* bitmap) {
+  const int tid = threadIdx.x, NT = blockDim.x;
+  for (int g = 0; g < C.ncg; g++) {
+    const int4 G = C.sp_cg[g];  // {first check, checks, slots, first slot descriptor}
+    const int2* __restrict__ sd = C.sp_desc + G.w;
+    const uint32_t ab0 = __ldg(&C.sp_absent[g]);
+    uint32_t bad = 0;
+    for (int t = tid; t < G.y; t += NT) {
+      const uint32_t keep = (t == 0) ? ~ab0 : ~0u;  // slots without an edge at t = 0
+      uint32_t p = 0;
+#pragma unroll
+      for (int i = 0; i < DCMAX; i++) {
+        if (i < G.z) {
+          const int u = slot_u(__ldg(&sd[i]), t, G.y);
+          p ^= (bitmap[u >> 5] >> (u & 31)) & (keep >> i);
+        }
+      }
+      bad |= p & 1u;
+    }
+    if (__syncthreads_or(bad)) return false;
+  }
+  return true;
 }
 
 // Fast sum-product update of check t of a row group whose D slots all hold an
@@ -210,8 +226,7 @@ __device__ __forceinline__ void app_put(float* app, int v, bool old_neg, float n
 template <int MSG16, int D, bool PART, class OM>
 __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
                                              typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om, bool first,
-                                             const LayerSmem& S, const int2* __restrict__ vg,
-                                             const int* __restrict__ ci, int vgs, int d) {
+                                             const LayerSmem& S, int d) {
   typedef MsgIO<MSG16> IO;
   float x[D], e[D];
 #pragma unroll
@@ -251,7 +266,7 @@ __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t,
   while (flips) {  // rare after the first iterations
     const int i = __ffs(flips) - 1;
     flips &= flips - 1;
-    flip_var(slot_u(__ldg(&sd[i]), t, nchk), S, vg, ci, vgs);
+    flip_var(slot_u(__ldg(&sd[i]), t, nchk), S);
   }
 }
 
@@ -268,7 +283,6 @@ template <int MSG16, int D, bool PART, class OM>
 __device__ __forceinline__ void spa_fast_rep_a(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
                                                typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om, bool first,
                                                uint32_t sync, float* dbuf, const LayerSmem& S,
-                                               const int2* __restrict__ vg, const int* __restrict__ ci, int vgs,
                                                int d) {
   typedef MsgIO<MSG16> IO;
   const uint32_t rep = sync | (sync << 1);  // slots inside a run
@@ -308,7 +322,7 @@ __device__ __forceinline__ void spa_fast_rep_a(const int2* __restrict__ sd, int 
       } else {
         const int v = slot_u(__ldg(&sd[i]), t, nchk);
         const float ov = app[v];
-        app_put(app, v, ov < 0.0f, __fadd_rn(ov, delta), S, vg, ci, vgs);
+        app_put(app, v, ov < 0.0f, __fadd_rn(ov, delta), S);
       }
     }
   }
@@ -316,8 +330,7 @@ __device__ __forceinline__ void spa_fast_rep_a(const int2* __restrict__ sd, int 
 
 template <int D>
 __device__ __forceinline__ void spa_fast_rep_b(const int2* __restrict__ sd, int t, int nchk, float* app,
-                                               uint32_t sync, const float* dbuf, const LayerSmem& S,
-                                               const int2* __restrict__ vg, const int* __restrict__ ci, int vgs) {
+                                               uint32_t sync, const float* dbuf, const LayerSmem& S) {
 #pragma unroll
   for (int i = 0; i < D; i++) {
     const bool head = ((sync >> i) & 1u) && !(i > 0 && ((sync >> (i - 1)) & 1u));
@@ -330,7 +343,7 @@ __device__ __forceinline__ void spa_fast_rep_b(const int2* __restrict__ sd, int 
         if (tj < 0) tj += nchk;
         nw = __fadd_rn(nw, dbuf[j * nchk + tj]);
       }
-      app_put(app, v, ov < 0.0f, nw, S, vg, ci, vgs);
+      app_put(app, v, ov < 0.0f, nw, S);
     }
   }
 }
@@ -347,8 +360,7 @@ template <int ALGO, int MSG16, int D, bool PART, class OM>
 __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
                                        typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om, bool first,
                                        float al, float be,
-                                       const LayerSmem& S, const int2* __restrict__ vg, const int* __restrict__ ci,
-                                       int vgs, int d) {
+                                       const LayerSmem& S, int d) {
   typedef MsgIO<MSG16> IO;
   float ap[D], o[D];
 #pragma unroll
@@ -394,7 +406,7 @@ __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int n
   while (flips) {  // rare after the first iterations
     const int i = __ffs(flips) - 1;
     flips &= flips - 1;
-    flip_var(slot_u(__ldg(&sd[i]), t, nchk), S, vg, ci, vgs);
+    flip_var(slot_u(__ldg(&sd[i]), t, nchk), S);
   }
 }
 
@@ -408,8 +420,7 @@ template <int ALGO, int MSG16, int D, bool PART, class OM>
 __device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
                                          typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om, bool first,
                                          float al, float be,
-                                         uint32_t sync, float* dbuf, const LayerSmem& S,
-                                         const int2* __restrict__ vg, const int* __restrict__ ci, int vgs, int d) {
+                                         uint32_t sync, float* dbuf, const LayerSmem& S, int d) {
   typedef MsgIO<MSG16> IO;
   const uint32_t rep = sync | (sync << 1);  // slots inside a run
   float ap[D], o[D];
@@ -452,7 +463,7 @@ __device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int
       dbuf[i * nchk + t] = delta;
     } else {
       const int v = slot_u(__ldg(&sd[i]), t, nchk);
-      app_put(app, v, ap[i] < 0.0f, __fadd_rn(ap[i], delta), S, vg, ci, vgs);
+      app_put(app, v, ap[i] < 0.0f, __fadd_rn(ap[i], delta), S);
     }
   }
 }
@@ -466,8 +477,7 @@ template <int ALGO, int MSG16, int DCMAX, class OM>
 __device__ __forceinline__ void general_row(const DecodeArgs& a, const int2* __restrict__ sd, int t, int nchk, int s0,
                                             float* app, typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om,
                                             bool first, int d, uint32_t ab, bool direct, float al, float be,
-                                            const LayerSmem& S, const int2* __restrict__ vg,
-                                            const int* __restrict__ vg_chk, int vgs, float (&wd)[DCMAX],
+                                            const LayerSmem& S, float (&wd)[DCMAX],
                                             int (&vv)[DCMAX]) {
   typedef MsgIO<MSG16> IO;
   float ap[DCMAX], o[DCMAX], w[DCMAX];
@@ -563,11 +573,11 @@ __device__ __forceinline__ void general_row(const DecodeArgs& a, const int2* __r
       const float out = IO::rt(w[i]);
       st_msg<MSG16>(c2v, s0 + i * nchk, out);
       if (ALGO == L_SPA_FAST) {
-        if (direct) app_put(app, vv[i], (apneg >> i) & 1u, ap[i] + out, S, vg, vg_chk, vgs);
+        if (direct) app_put(app, vv[i], (apneg >> i) & 1u, ap[i] + out, S);
         else wd[i] = out - o[i];
       } else {
         const float dl = __fsub_rn(out, o[i]);  // delta
-        if (direct) app_put(app, vv[i], (apneg >> i) & 1u, __fadd_rn(ap[i], dl), S, vg, vg_chk, vgs);
+        if (direct) app_put(app, vv[i], (apneg >> i) & 1u, __fadd_rn(ap[i], dl), S);
         else wd[i] = dl;
       }
     }
@@ -593,7 +603,7 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
                                                    typename MsgIO<MSG16>::T* __restrict__ c2v, const LayerSmem& S,
                                                    int maxit, int& it, int& converged, Stage& stg, int* abort) {
   typedef MsgIO<MSG16> IO;
-  const int tid = threadIdx.x, vgs = C.vgs, ncg = C.ncg;
+  const int tid = threadIdx.x, ncg = C.ncg;
   // stride of the loops over a thread's checks (one pass without MULTI)
   const int NT = MULTI ? (int)blockDim.x : (1 << 30);
   const int4* __restrict__ cgp = C.cg;
@@ -601,8 +611,6 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
   const uint32_t* __restrict__ cgs = C.cg_sync;
   const int2* __restrict__ sdesc = C.sp_desc;
   const uint32_t* __restrict__ absent = C.sp_absent;
-  const int2* __restrict__ vg = C.sp_vg;
-  const int* __restrict__ vg_chk = C.sp_ci;
   it = 0;
   converged = 0;
   // fused row paths: every algorithm but the exact sum-product
@@ -671,22 +679,18 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
           const int sc = G.w + tc;
           if constexpr (ALGO == L_SPA_FAST) {
             if (d == DCMAX)
-              spa_fast_rep_a<MSG16, DCMAX, false>(sd, tc, nchk, sc, app, c2v, omc, first, sync, S.dbuf, S, vg, vg_chk,
-                                                  vgs, d);
+              spa_fast_rep_a<MSG16, DCMAX, false>(sd, tc, nchk, sc, app, c2v, omc, first, sync, S.dbuf, S, d);
             else
-              spa_fast_rep_a<MSG16, DCMAX, true>(sd, tc, nchk, sc, app, c2v, omc, first, sync, S.dbuf, S, vg, vg_chk,
-                                                 vgs, d);
+              spa_fast_rep_a<MSG16, DCMAX, true>(sd, tc, nchk, sc, app, c2v, omc, first, sync, S.dbuf, S, d);
           } else if constexpr (kFused) {
             if (d == DCMAX)
-              ms_rep_a<ALGO, MSG16, DCMAX, false>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, sync, S.dbuf, S, vg,
-                                                  vg_chk, vgs, d);
+              ms_rep_a<ALGO, MSG16, DCMAX, false>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, sync, S.dbuf, S, d);
             else
-              ms_rep_a<ALGO, MSG16, DCMAX, true>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, sync, S.dbuf, S, vg,
-                                                 vg_chk, vgs, d);
+              ms_rep_a<ALGO, MSG16, DCMAX, true>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, sync, S.dbuf, S, d);
           }
         }
         __syncthreads();
-        for (int tc = tid; tc < nchk; tc += NT) spa_fast_rep_b<DCMAX>(sd, tc, nchk, app, sync, S.dbuf, S, vg, vg_chk, vgs);
+        for (int tc = tid; tc < nchk; tc += NT) spa_fast_rep_b<DCMAX>(sd, tc, nchk, app, sync, S.dbuf, S);
       } else if (sync == 0) {
         for (int tc = tid; tc < nchk; tc += NT) {
           const OM omc = old_of(tc);
@@ -695,20 +699,19 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
           if (kFused && d >= 2 && d <= DCMAX && ab == 0) {
             if constexpr (ALGO == L_SPA_FAST) {
               if (d == DCMAX)
-                spa_fast_row<MSG16, DCMAX, false>(sd, tc, nchk, sc, app, c2v, omc, first, S, vg, vg_chk, vgs, d);
+                spa_fast_row<MSG16, DCMAX, false>(sd, tc, nchk, sc, app, c2v, omc, first, S, d);
               else
-                spa_fast_row<MSG16, DCMAX, true>(sd, tc, nchk, sc, app, c2v, omc, first, S, vg, vg_chk, vgs, d);
+                spa_fast_row<MSG16, DCMAX, true>(sd, tc, nchk, sc, app, c2v, omc, first, S, d);
             } else if constexpr (kFused) {
               if (d == DCMAX)
-                ms_row<ALGO, MSG16, DCMAX, false>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, S, vg, vg_chk, vgs, d);
+                ms_row<ALGO, MSG16, DCMAX, false>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, S, d);
               else
-                ms_row<ALGO, MSG16, DCMAX, true>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, S, vg, vg_chk, vgs, d);
+                ms_row<ALGO, MSG16, DCMAX, true>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, S, d);
             }
           } else {
             float wd[DCMAX];
             int vd[DCMAX];
-            general_row<ALGO, MSG16, DCMAX>(a, sd, tc, nchk, sc, app, c2v, omc, first, d, ab, true, al, be, S, vg,
-                                           vg_chk, vgs, wd, vd);
+            general_row<ALGO, MSG16, DCMAX>(a, sd, tc, nchk, sc, app, c2v, omc, first, d, ab, true, al, be, S, wd, vd);
           }
         }
       } else if (!MULTI || NT >= nchk) {
@@ -718,8 +721,7 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
         int vd[DCMAX];
         if (act) {
           const uint32_t ab = (t == 0) ? __ldg(&absent[g]) : 0u;
-          general_row<ALGO, MSG16, DCMAX>(a, sd, t, nchk, s0, app, c2v, om, first, d, ab, false, al, be, S, vg,
-                                         vg_chk, vgs, wd, vd);
+          general_row<ALGO, MSG16, DCMAX>(a, sd, t, nchk, s0, app, c2v, om, first, d, ab, false, al, be, S, wd, vd);
         }
         __syncthreads();  // all pre-layer APP reads done
 #pragma unroll
@@ -728,7 +730,7 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
             if (act && vd[i] >= 0) {
               const int v = vd[i];
               const float ov = app[v];
-              app_put(app, v, ov < 0.0f, __fadd_rn(ov, wd[i]), S, vg, vg_chk, vgs);
+              app_put(app, v, ov < 0.0f, __fadd_rn(ov, wd[i]), S);
             }
             if ((sync >> i) & 1u) __syncthreads();
           }
@@ -742,7 +744,7 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
           int vd[DCMAX];
           const uint32_t ab = (tc == 0) ? __ldg(&absent[g]) : 0u;
           general_row<ALGO, MSG16, DCMAX>(a, sd, tc, nchk, G.w + tc, app, c2v, old_of(tc), first, d, ab, false, al, be,
-                                         S, vg, vg_chk, vgs, wd, vd);
+                                         S, wd, vd);
 #pragma unroll
           for (int i = 0; i < DCMAX; i++)
             if (i < d && vd[i] >= 0) S.dbuf[i * nchk + tc] = wd[i];
@@ -754,7 +756,7 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
             if ((ab >> i) & 1u) continue;
             const int v = slot_u(__ldg(&sd[i]), tc, nchk);
             const float ov = app[v];
-            app_put(app, v, ov < 0.0f, __fadd_rn(ov, S.dbuf[i * nchk + tc]), S, vg, vg_chk, vgs);
+            app_put(app, v, ov < 0.0f, __fadd_rn(ov, S.dbuf[i * nchk + tc]), S);
           }
           if ((sync >> i) & 1u) __syncthreads();
         }
@@ -767,13 +769,13 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
       }
     }
     ++it;
-    const int unsat = *S.unsat;
-    if (a.early_stop && unsat == 0) {
+    // the syndrome after each iteration (early stop) or after the last one; the
+    // barrier ending the last row group ordered every bitmap toggle before it
+    if ((a.early_stop || it >= maxit) && syndrome_zero<DCMAX>(C, S.bitmap)) {
       converged = 1;
       break;
     }
     if (it >= maxit) break;
-    __syncthreads();  // s_unsat read by all before the next iteration's updates
   }
 }
 
@@ -783,17 +785,15 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
   typedef MsgIO<MSG16> IO;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ long long s_frame;
-  __shared__ int s_unsat;
   __shared__ int s_abort;
   __shared__ DevCode C;
   uint32_t* bitmap = (uint32_t*)smem_raw;
-  uint32_t* chkpar = bitmap + a.bitmap_words;
-  float* smem_app = (float*)(smem_raw + (((a.bitmap_words + a.parity_words) * 4 + 15) & ~15));
+  float* smem_app = (float*)(smem_raw + ((a.bitmap_words * 4 + 15) & ~15));
   char* work = a.work + (long long)blockIdx.x * a.work_stride;
   MsgT* __restrict__ c2v = (MsgT*)work;
   float* gapp = (float*)(work + a.app_offset);
   const int tid = threadIdx.x, NT = blockDim.x;
-  LayerSmem S{bitmap, chkpar, &s_unsat, a.lay_dbuf_floats ? (float*)(smem_raw + a.lay_dbuf_off) : nullptr};
+  LayerSmem S{bitmap, a.lay_dbuf_floats ? (float*)(smem_raw + a.lay_dbuf_off) : nullptr};
   Stage stg{};
   if constexpr (STG) {
     stg.buf = (uint32_t)__cvta_generic_to_shared(smem_raw + a.lay_stage_off);
@@ -812,7 +812,6 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
       const long long q = (long long)atomicAdd(a.queue, 1ull);
       const long long nq = a.frames_dev ? *a.frames_dev : a.frames;  // queue entries
       s_frame = (q < nq) ? (a.order != nullptr ? a.order[q] : q) : -1;
-      s_unsat = 0;
     }
     __syncthreads();
     const long long f = s_frame;
@@ -828,10 +827,7 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
     }
     if (tid == 0) C = a.codes[cid];
     __syncthreads();
-    const int n = C.n, m = C.m;
-    const int4* __restrict__ spcg = C.sp_cg;
-    const int2* __restrict__ sdesc = C.sp_desc;
-    const uint32_t* __restrict__ absent = C.sp_absent;
+    const int n = C.n;
     const int* __restrict__ u2v = C.sp_u2v;
     const float* __restrict__ llr = a.llr + (a.llr_off ? a.llr_off[f] : f * (long long)n);
     const int maxit = a.max_iter_arr ? a.max_iter_arr[f] : a.max_iter;
@@ -865,30 +861,6 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
       if ((tid & 31) == 0 && u < n) bitmap[u >> 5] = b;
     }
     __syncthreads();
-    // check parities and the unsatisfied count
-    {
-      int cnt = 0;
-      for (int base = 0; base < m; base += NT) {
-        const int cc = base + tid;
-        uint32_t p = 0;
-        if (cc < m) {
-          const int g = C.chk_cg[cc];
-          const int4 G = spcg[g];
-          const int t = cc - G.x;
-          const uint32_t ab = t == 0 ? __ldg(&absent[g]) : 0u;
-          for (int i = 0; i < G.z; i++) {
-            const int u = slot_u(__ldg(&sdesc[G.w + i]), t, G.y);
-            if (!((ab >> i) & 1u)) p ^= (bitmap[u >> 5] >> (u & 31)) & 1u;
-          }
-        }
-        cnt += (int)p;
-        const unsigned b = __ballot_sync(0xffffffffu, p);
-        if ((tid & 31) == 0 && cc < m) chkpar[cc >> 5] = b;
-      }
-      atomicAdd(&s_unsat, cnt);
-    }
-    __syncthreads();
-
     int it = 0, converged = 0;
     if constexpr (DCMAX > 0) {
       layered_iterations<ALGO, MSG16, DCMAX, STG, (MAXT < 384)>(a, C, app, c2v, S, maxit, it, converged, stg,
@@ -923,7 +895,6 @@ __global__ void __launch_bounds__(MAXT, MINB) bp_layered_kernel(const DecodeArgs
       __syncthreads();
       if (s_abort) return;
     }
-    if (!converged) converged = (s_unsat == 0);
 
     if (mo) {
       const int wn = (n + 31) >> 5;
