@@ -375,13 +375,10 @@ __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int n
     if (PART && i >= d) continue;
     const float w = __fsub_rn(ap[i], o[i]);
     const float ax = fabsf(w);
-    if (ax < m1) {
-      m2 = m1;
-      m1 = ax;
-      i1 = i;
-    } else if (ax < m2) {
-      m2 = ax;
-    }
+    // the two smallest magnitudes and the first argmin, branch-free
+    i1 = (ax < m1) ? i : i1;
+    m2 = fminf(m2, fmaxf(m1, ax));
+    m1 = fminf(m1, ax);
     neg |= (uint32_t)(w < 0.0f) << i;
     apneg |= (uint32_t)(ap[i] < 0.0f) << i;
   }
@@ -391,14 +388,22 @@ __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int n
     mag1 = __fmul_rn(al, d1 > 0.0f ? d1 : 0.0f);
     mag2 = __fmul_rn(al, d2 > 0.0f ? d2 : 0.0f);
   }
+  // every message is +-mag1 or +-mag2: round the two through the message type
+  // once (the rounding is odd-symmetric, so the sign can follow)
+  const float r1 = IO::rt(mag1), r2 = IO::rt(mag2);
   const uint32_t negp = __popc(neg) & 1u;
   uint32_t flips = 0;
 #pragma unroll
   for (int i = 0; i < D; i++) {
     if (PART && i >= d) continue;
-    const float mag = (i == i1) ? mag2 : mag1;
-    const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
-    st_msg<MSG16>(c2v, s0 + i * nchk, out);
+    const uint32_t sflip = ((neg >> i) ^ negp) & 1u;
+    const float out = __uint_as_float(__float_as_uint((i == i1) ? r2 : r1) ^ (sflip << 31));
+    if constexpr (MSG16) {
+      const uint32_t h = (i == i1) ? __half_as_ushort(__float2half_rn(r2)) : __half_as_ushort(__float2half_rn(r1));
+      __stcs((unsigned short*)c2v + s0 + i * nchk, (unsigned short)(h ^ (sflip << 15)));
+    } else {
+      st_msg<MSG16>(c2v, s0 + i * nchk, out);
+    }
     const float nw = __fadd_rn(ap[i], __fsub_rn(out, o[i]));
     app[slot_u(__ldg(&sd[i]), t, nchk)] = nw;
     flips |= (uint32_t)(((apneg >> i) & 1u) != (uint32_t)(nw < 0.0f)) << i;
