@@ -124,6 +124,7 @@ def main(argv=None):
     if a.weights:
         tr.load(a.weights)
         steps = tr.step_no
+        lo, hi = tr.ebn0_range  # the checkpoint's training range
     else:
         t0 = time.time()
         tr.train(steps, log_every=max(1, steps // 10), log=lambda s: print(s, flush=True))
@@ -172,7 +173,8 @@ def main(argv=None):
         return (cross[x] - cross[y]) if cross.get(x) is not None and cross.get(y) is not None else None
     summary = dict(
         code=f"dvbt2-{a.frame}-{a.rate}", n=code.n(), k=code.k(), learned_iters=a.iters, schedule=a.schedule,
-        train=dict(frames=steps * a.batch, batch=a.batch, ebn0=[lo, hi], lr=a.lr, seconds=round(train_s, 2),
+        train=dict(frames=tr.frame_counter if a.weights else steps * a.batch, ebn0=[lo, hi], lr=a.lr,
+                   seconds=round(train_s, 2),
                    final_loss=tr.history[-1] if tr.history else None, loaded=a.weights),
         target_fer=a.target_fer, ebn0_at_target=cross,
         gap_db_learned_vs_spa50=diff("learned", "spa50"),
