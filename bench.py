@@ -550,10 +550,12 @@ class LearnedScale:
                    "plain_bp": plain}
 
     def host_step_factory(self):
-        """Pinned host LLRs copied in, the fallback call, results copied out.
-        Under torchrun (several ranks on one host) each rank's end-to-end step
-        covers its first 16384 frames, so that the pinned host buffers of all
-        ranks stay a few GB each."""
+        """The fallback call on pinned host memory: the library copies the LLRs
+        in, decodes (chunks whose copies overlap the decoding of the previous
+        chunk) and copies the results out before it returns.  Under torchrun
+        (several ranks on one host) each rank's end-to-end step covers its
+        first 16384 frames, so that the pinned host buffers of all ranks stay
+        a few GB each."""
         torch = self.torch
         world = int(os.environ.get("WORLD_SIZE", "1"))
         F = self.frames if world == 1 else min(self.frames, 16384)
@@ -561,20 +563,14 @@ class LearnedScale:
         self.e2e_frames = F
         h_llr = torch.empty((F, n), dtype=torch.float32, pin_memory=True)
         h_llr.copy_(self.llr[:F])
-        d_llr = torch.empty((F, n), dtype=torch.float32, device=self.llr.device)
-        h_msg = torch.empty((F, wk), dtype=torch.int64, pin_memory=True)
-        h_it = torch.empty(F, dtype=torch.int32, pin_memory=True)
-        h_ok = torch.empty(F, dtype=torch.uint8, pin_memory=True)
-        state = {"out": None}
+        out = dict(msg=torch.empty((F, wk), dtype=torch.int64, pin_memory=True),
+                   iters=torch.empty(F, dtype=torch.int32, pin_memory=True),
+                   conv=torch.empty(F, dtype=torch.uint8, pin_memory=True),
+                   synd_ok=torch.empty(F, dtype=torch.uint8, pin_memory=True))
 
         def host_step():
-            d_llr.copy_(h_llr, non_blocking=True)
-            state["out"] = o = self.nms.decode_with_fallback(self.spa, d_llr, self.T, 50, out=state["out"])
-            h_msg.copy_(o["msg"], non_blocking=True)
-            h_it.copy_(o["iters"], non_blocking=True)
-            h_ok.copy_(o["synd_ok"], non_blocking=True)
-            torch.cuda.synchronize()
-        return host_step, F * n * 4, F * (wk * 8 + 4 + 1)
+            self.nms.decode_with_fallback(self.spa, h_llr, self.T, 50, out=out)
+        return host_step, F * n * 4, F * (wk * 8 + 4 + 1 + 1)
 
 
 def shannon_limit(rate):

@@ -102,7 +102,8 @@ extern "C" {
     pub fn gf2c_decode_batch_fallback(primary: *mut gf2c_decoder, fallback: *mut gf2c_decoder, llr: *const f32,
                                       frames: i64, max_iter_primary: i32, max_iter_fallback: i32,
                                       msg_bits: *mut u64, iterations: *mut i32, converged: *mut u8,
-                                      syndrome_ok: *mut u8, fallback_count: *mut i64, stream: *mut c_void) -> i32;
+                                      syndrome_ok: *mut u8, fallback_count: *mut i64, mem: i32,
+                                      stream: *mut c_void) -> i32;
     pub fn gf2c_decode_mixed(dec: *mut gf2c_decoder, llr: *const f32, llr_offset: *const i64, code_id: *const i32,
                              max_iter: *const i32, frames: i64, msg_bits: *mut u64, msg_offset: *const i64,
                              iterations: *mut i32, converged: *mut u8, syndrome_ok: *mut u8, use_graph: i32,

@@ -240,6 +240,43 @@ impl CudaLdpcDecoder {
             })
             .collect()
     }
+
+    /// `decode_batch` with a fallback decoder (no counterpart in the
+    /// reference): this decoder on every frame, then `fallback` (a layered
+    /// decoder of the same code, e.g. sum-product) on the frames whose
+    /// syndrome still fails, the list kept on the device.  Returns the results
+    /// and the number of frames re-decoded.
+    pub fn decode_batch_with_fallback(&mut self, fallback: &mut CudaLdpcDecoder, llr_blocks: &[Vec<Llr>],
+                                      max_iterations: usize, fallback_iterations: usize)
+                                      -> (Vec<DecoderResult>, usize) {
+        let (n, k, f) = (self.code.n, self.code.k, llr_blocks.len());
+        if f == 0 {
+            return (Vec::new(), 0);
+        }
+        let mut llr = Vec::with_capacity(f * n);
+        for b in llr_blocks {
+            assert_eq!(b.len(), n, "LLR length must equal n");
+            llr.extend(b.iter().map(|l| l.value()));
+        }
+        let wk = words(k);
+        let mut bits = vec![0u64; f * wk];
+        let mut iters = vec![0i32; f];
+        let (mut conv, mut synd) = (vec![0u8; f], vec![0u8; f]);
+        let mut redecoded = 0i64;
+        check(unsafe {
+            ffi::gf2c_decode_batch_fallback(self.raw, fallback.raw, llr.as_ptr(), f as i64, max_iterations as i32,
+                                            fallback_iterations as i32, bits.as_mut_ptr(), iters.as_mut_ptr(),
+                                            conv.as_mut_ptr(), synd.as_mut_ptr(), &mut redecoded,
+                                            ffi::GF2C_MEM_HOST, ptr::null_mut())
+        });
+        let results = (0..f)
+            .map(|i| {
+                DecoderResult::new(BitVec::from_words(bits[i * wk..(i + 1) * wk].to_vec(), k), iters[i] as usize,
+                                   conv[i] != 0, synd[i] != 0)
+            })
+            .collect();
+        (results, redecoded as usize)
+    }
 }
 
 impl Drop for CudaLdpcDecoder {

@@ -96,7 +96,7 @@ def _load():
     L.gf2c_decoder_create_multi.argtypes = [_vp, _i32, ctypes.POINTER(DecoderOpts), ctypes.POINTER(_vp)]
     L.gf2c_decoder_destroy.argtypes = [_vp]
     L.gf2c_decode_batch.argtypes = [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _vp]
-    L.gf2c_decode_batch_fallback.argtypes = [_vp, _vp, _vp, _i64, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.gf2c_decode_batch_fallback.argtypes = [_vp, _vp, _vp, _i64, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _vp]
     L.gf2c_decode_mixed.argtypes = [_vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _vp]
     L.gf2c_decoder_last_launches.argtypes = [_vp, ctypes.POINTER(_i32)]
     L.gf2c_decode_batch_noalloc.argtypes = [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp]

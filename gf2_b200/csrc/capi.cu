@@ -77,8 +77,9 @@ struct gf2c_decoder {
   std::map<GraphKey, cudaGraphExec_t> graphs;
   cudaStream_t gstream = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
-  // pipelined host-memory batches: a second stream with its own workspace and queue
-  cudaStream_t pstream = nullptr;
+  // pipelined host-memory batches: a second decode stream with its own
+  // workspace and queue, and a stream that issues the input copies
+  cudaStream_t pstream = nullptr, cstream = nullptr;
   cudaEvent_t pev_fork = nullptr, pev_join = nullptr, pev_copy[2] = {nullptr, nullptr};
   DevBuf work2, queue2;
   // mixed batches: rank of each code in the frame order (longest codes first), frame order buffer
@@ -93,10 +94,11 @@ struct gf2c_decoder {
       cudaStreamSynchronize(gstream);
       cudaStreamDestroy(gstream);
     }
-    if (pstream) {
-      cudaStreamSynchronize(pstream);
-      cudaStreamDestroy(pstream);
-    }
+    for (cudaStream_t ps : {pstream, cstream})
+      if (ps) {
+        cudaStreamSynchronize(ps);
+        cudaStreamDestroy(ps);
+      }
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
     for (cudaEvent_t e : {pev_fork, pev_join, pev_copy[0], pev_copy[1]})
@@ -621,15 +623,28 @@ static int check_status(gf2c_decoder* d, cudaStream_t st) {
   return GF2C_OK;
 }
 
-// The second stream, workspace and queue of the pipelined host-memory path
-// (made on first use; false where they cannot be had, and the call then runs
-// unpipelined).
+// Chunk sizes of the pipelined host-memory paths: one wave of frames first
+// (the copy that nothing overlaps is short), then doubling up to an eighth of
+// the batch, so that each copy is done before the SMs run out of work both when
+// decoding is much slower than the copy and when it runs at about the copy's
+// speed (the last chunk's decode, after the last copy, is then short); a
+// remainder below one wave joins the last chunk.
+static int64_t chunk_frames(int64_t want, int64_t left, int64_t wave) {
+  const int64_t nf = std::min(want, left);
+  return (left - nf < wave) ? left : nf;
+}
+static int64_t chunk_cap(int64_t frames, int64_t wave) { return std::max(wave, (frames + 7) / 8); }
+
+// The second decode stream, its workspace and queue, and the copy stream of
+// the pipelined host-memory path (made on first use; false where they cannot
+// be had, and the call then runs unpipelined).
 static bool pipeline_ready(gf2c_decoder* d) {
-  if (!d->pstream && cudaStreamCreateWithFlags(&d->pstream, cudaStreamNonBlocking) != cudaSuccess) {
-    d->pstream = nullptr;
-    cudaGetLastError();
-    return false;
-  }
+  for (cudaStream_t* ps : {&d->pstream, &d->cstream})
+    if (!*ps && cudaStreamCreateWithFlags(ps, cudaStreamNonBlocking) != cudaSuccess) {
+      *ps = nullptr;
+      cudaGetLastError();
+      return false;
+    }
   for (cudaEvent_t* e : {&d->pev_fork, &d->pev_join, &d->pev_copy[0], &d->pev_copy[1]})
     if (!*e && cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) {
       *e = nullptr;
@@ -674,29 +689,31 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
     return rc;
   if (beliefs && (rc = dec->s_bel.ensure(bl))) return rc;
   // Large batches: chunks of frames alternating between the caller's stream and
-  // a second stream, each stream running copy in, decode and copy out of its
-  // chunks in order.  Copies overlap the decode of the other stream's chunk,
-  // and a chunk's decode starts on the SMs that the previous chunk's last
-  // frames leave free (each stream has its own workspace and frame queue).
+  // a second stream, each stream running decode and copy out of its chunks in
+  // order, while a copy stream brings the chunks in back to back (the staging
+  // buffer holds the whole batch, so no copy waits for a decode).  A chunk's
+  // decode waits for its own copy only and starts on the SMs that the previous
+  // chunk's last frames leave free (each stream has its own workspace and
+  // frame queue).
   const int64_t chunk = std::max<int64_t>(dec->grid, (frames + 7) / 8);
   if (frames >= 2 * chunk && bl >= ((size_t)64 << 20) && pipeline_ready(dec)) {
     GF2C_CUDA(cudaEventRecord(dec->pev_fork, st));
     GF2C_CUDA(cudaStreamWaitEvent(dec->pstream, dec->pev_fork, 0));
-    // chunk sizes: one wave of frames first (the copy that nothing overlaps is
-    // short), then doubling, so that each copy is done before the SMs run out
-    // of decoding work; a remainder below the next size joins the last chunk
+    GF2C_CUDA(cudaStreamWaitEvent(dec->cstream, dec->pev_fork, 0));
     int chunks = 0, launches = 0;
-    for (int64_t f0 = 0, nf = 0, want = dec->grid; f0 < frames; f0 += nf, chunks++, want *= 2) {
-      nf = std::min(want, frames - f0);
-      if (frames - f0 - nf < want) nf = frames - f0;
+    const int64_t cap = chunk_cap(frames, dec->grid);
+    for (int64_t f0 = 0, nf = 0, want = dec->grid; f0 < frames; f0 += nf, chunks++, want = std::min(2 * want, cap)) {
+      nf = chunk_frames(want, frames - f0, dec->grid);
       const int slot = chunks & 1;
       cudaStream_t s = slot ? dec->pstream : st;
       const size_t ln = (size_t)nf * h.n * 4, lo = (size_t)f0 * h.n * 4;
       const size_t mn = (size_t)nf * wk * 8, mo = (size_t)f0 * wk * 8;
-      // input copies in chunk order, one at a time (the first decode waits for the first copy only)
-      if (chunks > 0) GF2C_CUDA(cudaStreamWaitEvent(s, dec->pev_copy[slot ^ 1], 0));
-      GF2C_CUDA(cudaMemcpyAsync((char*)dec->s_llr.p + lo, (const char*)llr + lo, ln, cudaMemcpyHostToDevice, s));
-      GF2C_CUDA(cudaEventRecord(dec->pev_copy[slot], s));
+      // input copies back to back on the copy stream (the staging buffer holds
+      // the whole batch), each chunk's decode waiting for its own copy only
+      GF2C_CUDA(cudaMemcpyAsync((char*)dec->s_llr.p + lo, (const char*)llr + lo, ln, cudaMemcpyHostToDevice,
+                                dec->cstream));
+      GF2C_CUDA(cudaEventRecord(dec->pev_copy[slot], dec->cstream));
+      GF2C_CUDA(cudaStreamWaitEvent(s, dec->pev_copy[slot], 0));
       DecodeArgs b = a;
       b.llr = (const float*)((char*)dec->s_llr.p + lo);
       b.msg = msg_bits ? (uint64_t*)((char*)dec->s_msg.p + mo) : nullptr;
@@ -743,56 +760,144 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
   return check_status(dec, st);
 }
 
+// One primary pass, failed-frame list and fallback pass over `frames` frames
+// whose arrays `a` points at, on stream `st` (slot: workspace and queue of the
+// pipelined host path); the list goes to `list`, its length to *cnt.
+static int fallback_passes(gf2c_decoder* primary, gf2c_decoder* fallback, DecodeArgs a, int64_t frames,
+                           int32_t max_iter_primary, int32_t max_iter_fallback, int64_t* list, long long* cnt,
+                           cudaStream_t st, int slot, int& launches) {
+  int rc, extra = 0;
+  // 1. the primary decoder on every frame
+  a.max_iter = max_iter_primary;
+  if ((rc = key_order(primary, a, frames, st, slot, extra))) return rc;
+  if ((rc = launch_decoder(primary, a, frames, st, slot))) return rc;
+  // 2. the frames it left failing, listed on the device
+  GF2C_CUDA(launch_failed_list(a.synd_ok, frames, list, cnt, st));
+  // 3. the fallback decoder on the listed frames (count read on the device)
+  DecodeArgs b = a;
+  b.max_iter = max_iter_fallback;
+  b.order = list;
+  b.frames_dev = cnt;
+  b.iters_add = max_iter_primary;
+  if ((rc = launch_decoder(fallback, b, frames, st, slot))) return rc;
+  launches = 3 + extra;
+  return GF2C_OK;
+}
+
 int gf2c_decode_batch_fallback(gf2c_decoder* primary, gf2c_decoder* fallback, const float* llr, int64_t frames,
                                int32_t max_iter_primary, int32_t max_iter_fallback, uint64_t* msg_bits,
                                int32_t* iterations, uint8_t* converged, uint8_t* syndrome_ok,
-                               int64_t* fallback_count, void* stream) {
+                               int64_t* fallback_count, int32_t mem, void* stream) {
   if (!primary || !fallback || frames < 0 || max_iter_primary < 0 || max_iter_fallback <= 0 || (frames > 0 && !llr))
     return set_error(GF2C_ERR_INVALID_ARG, "bad arguments");
+  int rc = check_mem(mem);
+  if (rc) return rc;
   if (primary->codes.size() != 1 || fallback->codes.size() != 1 ||
       primary->codes[0]->h->serial != fallback->codes[0]->h->serial)
     return set_error(GF2C_ERR_INVALID_ARG, "both decoders must decode the same single code");
   if (fallback->opts.schedule != GF2C_SCHED_LAYERED)
     return set_error(GF2C_ERR_UNSUPPORTED, "the fallback decoder must use the layered schedule");
-  if (frames == 0) return GF2C_OK;
-  cudaStream_t st = (cudaStream_t)stream;
-  int rc;
-  uint8_t* so = syndrome_ok;
-  if (!so) {
-    if ((rc = primary->s_so.ensure((size_t)frames))) return rc;
-    so = (uint8_t*)primary->s_so.p;
+  if (frames == 0) {
+    if (fallback_count && mem == GF2C_MEM_HOST) *fallback_count = 0;
+    return GF2C_OK;
   }
-  if ((rc = primary->fb_list.ensure((size_t)frames * 8)) || (rc = primary->fb_count.ensure(64))) return rc;
-  // 1. the primary decoder on every frame
-  DecodeArgs a{};
-  a.max_iter = max_iter_primary;
-  a.llr = llr;
-  a.msg = msg_bits;
-  a.iters = iterations;
-  a.conv = converged;
-  a.synd_ok = so;
-  int extra = 0;
-  if ((rc = key_order(primary, a, frames, st, 0, extra))) return rc;
-  if ((rc = launch_decoder(primary, a, frames, st))) return rc;
-  const int launches = primary->last_launches + extra;
-  // 2. the frames it left failing, listed on the device
-  long long* cnt = (long long*)primary->fb_count.p;
-  GF2C_CUDA(launch_failed_list(so, frames, (int64_t*)primary->fb_list.p, cnt, st));
-  // 3. the fallback decoder on the listed frames (count read on the device)
-  DecodeArgs b{};
-  b.max_iter = max_iter_fallback;
-  b.llr = llr;
-  b.msg = msg_bits;
-  b.iters = iterations;
-  b.conv = converged;
-  b.synd_ok = so;
-  b.order = (const int64_t*)primary->fb_list.p;
-  b.frames_dev = cnt;
-  b.iters_add = max_iter_primary;
-  if ((rc = launch_decoder(fallback, b, frames, st))) return rc;
-  if (fallback_count)
-    GF2C_CUDA(cudaMemcpyAsync(fallback_count, cnt, sizeof(long long), cudaMemcpyDeviceToDevice, st));
-  primary->last_launches = launches + 2;
+  cudaStream_t st = (cudaStream_t)stream;
+  int launches = 0;
+  if (mem == GF2C_MEM_DEVICE) {
+    uint8_t* so = syndrome_ok;
+    if (!so) {
+      if ((rc = primary->s_so.ensure((size_t)frames))) return rc;
+      so = (uint8_t*)primary->s_so.p;
+    }
+    if ((rc = primary->fb_list.ensure((size_t)frames * 8)) || (rc = primary->fb_count.ensure(64))) return rc;
+    DecodeArgs a{};
+    a.llr = llr;
+    a.msg = msg_bits;
+    a.iters = iterations;
+    a.conv = converged;
+    a.synd_ok = so;
+    long long* cnt = (long long*)primary->fb_count.p;
+    if ((rc = fallback_passes(primary, fallback, a, frames, max_iter_primary, max_iter_fallback,
+                              (int64_t*)primary->fb_list.p, cnt, st, 0, launches)))
+      return rc;
+    if (fallback_count)
+      GF2C_CUDA(cudaMemcpyAsync(fallback_count, cnt, sizeof(long long), cudaMemcpyDeviceToDevice, st));
+    primary->last_launches = launches;
+    return GF2C_OK;
+  }
+  // Host memory: the batch is staged in the primary decoder's buffers.  Large
+  // batches go in chunks alternating between the caller's stream and a second
+  // stream, as in gf2c_decode_batch, with the input copies issued back to back
+  // on a copy stream.  Every chunk has its own list and count.
+  const HostCode& h = *primary->codes[0]->h;
+  const int wk = (int)((h.k + 63) / 64);
+  const size_t bl = (size_t)frames * h.n * 4, bm = (size_t)frames * wk * 8;
+  if ((rc = primary->s_llr.ensure(bl)) || (rc = primary->s_msg.ensure(bm)) ||
+      (rc = primary->s_it.ensure((size_t)frames * 4)) || (rc = primary->s_cv.ensure((size_t)frames)) ||
+      (rc = primary->s_so.ensure((size_t)frames)) || (rc = primary->fb_list.ensure((size_t)frames * 8)) ||
+      (rc = primary->fb_count.ensure(64 * 8)))
+    return rc;
+  const int64_t wave = std::max(primary->grid, fallback->grid);
+  const bool pipe = frames >= 3 * wave && bl >= ((size_t)64 << 20) && pipeline_ready(primary) &&
+                    pipeline_ready(fallback);
+  if (pipe) {
+    GF2C_CUDA(cudaEventRecord(primary->pev_fork, st));
+    GF2C_CUDA(cudaStreamWaitEvent(primary->pstream, primary->pev_fork, 0));
+    GF2C_CUDA(cudaStreamWaitEvent(primary->cstream, primary->pev_fork, 0));
+  }
+  int chunks = 0;
+  const int64_t cap = chunk_cap(frames, wave);
+  for (int64_t f0 = 0, nf = 0, want = pipe ? wave : frames; f0 < frames;
+       f0 += nf, chunks++, want = std::min(2 * want, cap)) {
+    nf = (chunks == 63) ? frames - f0 : chunk_frames(want, frames - f0, wave);
+    const int slot = pipe ? (chunks & 1) : 0;
+    cudaStream_t s = slot ? primary->pstream : st;
+    const size_t ln = (size_t)nf * h.n * 4, lo = (size_t)f0 * h.n * 4;
+    const size_t mn = (size_t)nf * wk * 8, mo = (size_t)f0 * wk * 8;
+    // input copies back to back on the copy stream, each chunk's passes
+    // waiting for its own copy only
+    if (pipe) {
+      GF2C_CUDA(cudaMemcpyAsync((char*)primary->s_llr.p + lo, (const char*)llr + lo, ln, cudaMemcpyHostToDevice,
+                                primary->cstream));
+      GF2C_CUDA(cudaEventRecord(primary->pev_copy[slot], primary->cstream));
+      GF2C_CUDA(cudaStreamWaitEvent(s, primary->pev_copy[slot], 0));
+    } else {
+      GF2C_CUDA(cudaMemcpyAsync((char*)primary->s_llr.p + lo, (const char*)llr + lo, ln, cudaMemcpyHostToDevice, s));
+    }
+    DecodeArgs a{};
+    a.llr = (const float*)((char*)primary->s_llr.p + lo);
+    a.msg = msg_bits ? (uint64_t*)((char*)primary->s_msg.p + mo) : nullptr;
+    a.iters = (int32_t*)primary->s_it.p + f0;
+    a.conv = (uint8_t*)primary->s_cv.p + f0;
+    a.synd_ok = (uint8_t*)primary->s_so.p + f0;
+    int nl = 0;
+    if ((rc = fallback_passes(primary, fallback, a, nf, max_iter_primary, max_iter_fallback,
+                              (int64_t*)primary->fb_list.p + f0, (long long*)primary->fb_count.p + chunks, s, slot,
+                              nl)))
+      return rc;
+    launches += nl;
+    if (msg_bits)
+      GF2C_CUDA(cudaMemcpyAsync((char*)msg_bits + mo, (char*)primary->s_msg.p + mo, mn, cudaMemcpyDeviceToHost, s));
+    if (iterations)
+      GF2C_CUDA(cudaMemcpyAsync(iterations + f0, (int32_t*)primary->s_it.p + f0, nf * 4, cudaMemcpyDeviceToHost, s));
+    if (converged)
+      GF2C_CUDA(cudaMemcpyAsync(converged + f0, (uint8_t*)primary->s_cv.p + f0, nf, cudaMemcpyDeviceToHost, s));
+    if (syndrome_ok)
+      GF2C_CUDA(cudaMemcpyAsync(syndrome_ok + f0, (uint8_t*)primary->s_so.p + f0, nf, cudaMemcpyDeviceToHost, s));
+  }
+  if (pipe) {
+    GF2C_CUDA(cudaEventRecord(primary->pev_join, primary->pstream));
+    GF2C_CUDA(cudaStreamWaitEvent(st, primary->pev_join, 0));
+  }
+  long long counts[64] = {0};
+  GF2C_CUDA(cudaMemcpyAsync(counts, primary->fb_count.p, sizeof(long long) * chunks, cudaMemcpyDeviceToHost, st));
+  primary->last_launches = launches;
+  if ((rc = check_status(primary, st)) || (rc = check_status(fallback, st))) return rc;
+  if (fallback_count) {
+    long long total = 0;
+    for (int c = 0; c < chunks; c++) total += counts[c];
+    *fallback_count = total;
+  }
   return GF2C_OK;
 }
 

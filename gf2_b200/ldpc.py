@@ -487,15 +487,43 @@ class LdpcDecoder:
         return out
 
     def decode_with_fallback(self, fallback, llr, max_iterations, fallback_iterations, out=None, stream=None):
-        """This decoder on every frame of a device batch, then `fallback` (a
-        layered decoder of the same code) on the frames whose syndrome still
-        fails, all on the device (gf2c_decode_batch_fallback).  Returns a dict
-        of device tensors; fallback_count [1] int64 = frames re-decoded."""
+        """This decoder on every frame of a batch, then `fallback` (a layered
+        decoder of the same code) on the frames whose syndrome still fails,
+        the list of those frames kept on the device
+        (gf2c_decode_batch_fallback).
+        Device batch (CUDA tensor [F, n] f32): asynchronous on `stream`; returns
+        a dict of device tensors, fallback_count [1] int64 = frames re-decoded.
+        Host batch (CPU tensor or numpy array [F, n] f32; pinned tensors copy
+        fastest): copied in, decoded (large batches in chunks whose copies
+        overlap decoding) and copied out before the call returns; returns CPU
+        tensors (numpy arrays for numpy input) and fallback_count as an int."""
         import torch
-        if llr.dtype != torch.float32 or not llr.is_cuda or llr.dim() != 2 or llr.shape[1] != self.n():
-            raise ValueError("llr must be a CUDA float32 tensor [frames, n]")
+        host_np = isinstance(llr, np.ndarray)
+        if host_np:
+            llr = torch.from_numpy(np.ascontiguousarray(llr, dtype=np.float32))
+        if llr.dtype != torch.float32 or llr.dim() != 2 or llr.shape[1] != self.n():
+            raise ValueError("llr must be a float32 tensor / array [frames, n]")
         llr = llr.contiguous()
         F, dev = llr.shape[0], llr.device
+        if not llr.is_cuda:
+            if out is None:
+                pin = llr.is_pinned()
+                out = dict(msg=torch.zeros((F, words(self.k())), dtype=torch.int64, pin_memory=pin),
+                           iters=torch.zeros(F, dtype=torch.int32, pin_memory=pin),
+                           conv=torch.zeros(F, dtype=torch.uint8, pin_memory=pin),
+                           synd_ok=torch.zeros(F, dtype=torch.uint8, pin_memory=pin))
+            for k in ("msg", "iters", "conv", "synd_ok"):
+                if out[k].is_cuda or not out[k].is_contiguous() or out[k].shape[0] != F:
+                    raise ValueError("host outputs must be contiguous CPU tensors of the batch's frames")
+            cnt = np.zeros(1, np.int64)
+            C.check(C.lib.gf2c_decode_batch_fallback(self._h, fallback._h, _ptr(llr), F, int(max_iterations),
+                                                     int(fallback_iterations), _ptr(out["msg"]), _ptr(out["iters"]),
+                                                     _ptr(out["conv"]), _ptr(out["synd_ok"]), _ptr(cnt),
+                                                     C.MEM_HOST, None))
+            out["fallback_count"] = int(cnt[0])
+            if host_np:
+                out = {k: (v.numpy() if hasattr(v, "numpy") else v) for k, v in out.items()}
+            return out
         if out is None:
             out = dict(msg=torch.zeros((F, words(self.k())), dtype=torch.int64, device=dev),
                        iters=torch.zeros(F, dtype=torch.int32, device=dev),
@@ -506,7 +534,7 @@ class LdpcDecoder:
         C.check(C.lib.gf2c_decode_batch_fallback(self._h, fallback._h, _ptr(llr), F, int(max_iterations),
                                                  int(fallback_iterations), _ptr(out["msg"]), _ptr(out["iters"]),
                                                  _ptr(out["conv"]), _ptr(out["synd_ok"]),
-                                                 _ptr(out["fallback_count"]), _stream_ptr(st)))
+                                                 _ptr(out["fallback_count"]), C.MEM_DEVICE, _stream_ptr(st)))
         return out
 
     def decode_iterative(self, llrs, max_iterations):

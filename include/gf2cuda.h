@@ -185,13 +185,18 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
  * from their LLRs with max_iter_fallback iterations, its results replacing
  * theirs (iterations = max_iter_primary + the fallback's count).  The list
  * and its length stay on the device: no host synchronisation between the
- * passes.  fallback_count (nullable, device int64): frames re-decoded.
- * Both decoders must decode the same code.  All pointers are device memory;
- * asynchronous on `stream`; 3 or 5 kernel launches. */
+ * passes.  fallback_count (nullable, int64): frames re-decoded.
+ * Both decoders must decode the same code.
+ *   mem == GF2C_MEM_DEVICE: every pointer is device memory (fallback_count
+ *     too); asynchronous on `stream`; 3 or 5 kernel launches.
+ *   mem == GF2C_MEM_HOST: every pointer is host memory (pinned memory copies
+ *     fastest); the batch is copied in, decoded and copied out, large batches
+ *     in chunks on two streams so that copies overlap decoding; returns when
+ *     the results are in host memory. */
 int gf2c_decode_batch_fallback(gf2c_decoder* primary, gf2c_decoder* fallback, const float* llr, int64_t frames,
                                int32_t max_iter_primary, int32_t max_iter_fallback, uint64_t* msg_bits,
                                int32_t* iterations, uint8_t* converged, uint8_t* syndrome_ok,
-                               int64_t* fallback_count, void* stream);
+                               int64_t* fallback_count, int32_t mem, void* stream);
 
 /* Mixed batch in one persistent launch: frame f uses code code_id[f] (index into the
  * codes given at creation), reads n[code] LLRs at llr + llr_offset[f], writes

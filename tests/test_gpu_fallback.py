@@ -54,3 +54,29 @@ def test_fallback_argument_checks(gpu):
         da.decode_with_fallback(db, llr, 5, 10)  # different codes
     with pytest.raises(g.Gf2cError):
         da.decode_with_fallback(flood, llr, 5, 10)  # fallback not layered
+
+
+@pytest.mark.parametrize("frames", [40, 1000])
+def test_fallback_host_memory_equals_device(gpu, frames):
+    """The host-memory call (pinned buffers; 1000 normal frames go in two
+    chunks on two streams) gives the device call's results and count."""
+    code = g.LdpcCode.dvb_t2_normal(g.CodeRate.Rate2_3)
+    L, T = code.layers(), 10
+    prim = g.LdpcDecoder(code, algorithm=g.ALGO_NMS, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16,
+                         nms_alpha=np.full((T, L), 0.8, np.float32), nms_beta=np.zeros((T, L), np.float32))
+    fb = g.LdpcDecoder(code, algorithm=g.ALGO_SPA_FAST, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16)
+    s2 = np.array([g.sigma2_from_ebn0(2.0 + 0.1 * (f % 4), code.rate()) for f in range(frames)])
+    _, _, llr = g.awgn_frames(code, 43, 0, frames, s2, device=gpu, want_info=False, want_cw=False)
+    d = prim.decode_with_fallback(fb, llr, T, 50)
+    torch.cuda.synchronize()
+    assert int(d["fallback_count"][0]) > 0
+    h_llr = llr.cpu().pin_memory()
+    h = prim.decode_with_fallback(fb, h_llr, T, 50)
+    assert h["fallback_count"] == int(d["fallback_count"][0])
+    for k in ("msg", "iters", "conv", "synd_ok"):
+        assert not h[k].is_cuda
+        assert torch.equal(h[k], d[k].cpu()), k
+    # numpy in, numpy out (pageable memory)
+    hn = prim.decode_with_fallback(fb, llr.cpu().numpy(), T, 50)
+    assert isinstance(hn["msg"], np.ndarray) and hn["fallback_count"] == h["fallback_count"]
+    assert (hn["msg"] == d["msg"].cpu().numpy()).all() and (hn["iters"] == d["iters"].cpu().numpy()).all()
