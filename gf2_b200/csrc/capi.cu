@@ -82,8 +82,11 @@ struct gf2c_decoder {
   cudaStream_t pstream = nullptr, cstream = nullptr;
   cudaEvent_t pev_fork = nullptr, pev_join = nullptr, pev_copy[2] = {nullptr, nullptr};
   DevBuf work2, queue2;
-  // mixed batches: rank of each code in the frame order (longest codes first), frame order buffer
-  DevBuf d_rank, d_order;
+  // mixed batches: rank of each code in the frame order (longest codes first),
+  // frame order buffer; host copy of the ranks and the per-chunk frame counts
+  // of the pipelined host-memory path
+  DevBuf d_rank, d_order, s_cnt;
+  std::vector<int32_t> h_rank;
   // single-code batches, hardest frames first: per-frame keys and order (one pair per stream slot)
   DevBuf d_key[2], d_korder[2];
   // fallback decoding: the frames this decoder left failing (list and count)
@@ -344,6 +347,7 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
     for (size_t r = 0; r < by.size(); r++) rank[by[r]] = (int32_t)r;
     if ((rc = d->d_rank.ensure(sizeof(int32_t) * rank.size()))) return rc;
     GF2C_CUDA(cudaMemcpy(d->d_rank.p, rank.data(), sizeof(int32_t) * rank.size(), cudaMemcpyHostToDevice));
+    d->h_rank = rank;
   }
 
   // NMS weights
@@ -996,6 +1000,78 @@ int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_of
       (rc = dec->s_off1.ensure(frames * 8)) || (rc = dec->s_off2.ensure(frames * 8)) ||
       (rc = dec->s_cid.ensure(frames * 4)) || (rc = dec->s_mit.ensure(frames * 4)))
     return rc;
+  // Large batches: chunks of frames in memory order, each chunk's LLRs brought
+  // in by the copy stream while earlier chunks decode on two streams (as in
+  // gf2c_decode_batch).  The frame order of a chunk (code by code, longest
+  // codes first, then by frame index, the ordering kernel's rule) is made on
+  // the host; the persistent kernel takes the chunk's frames from it.
+  const int64_t wave = dec->grid;
+  if (ordered && frames >= 3 * wave && (size_t)llr_total * 4 >= ((size_t)64 << 20) && pipeline_ready(dec) &&
+      dec->s_cnt.ensure(64 * 8) == GF2C_OK) {
+    std::vector<int64_t> mem((size_t)frames), ord((size_t)frames);
+    for (int64_t f = 0; f < frames; f++) mem[f] = f;
+    std::stable_sort(mem.begin(), mem.end(), [&](int64_t x, int64_t y) { return llr_offset[x] < llr_offset[y]; });
+    std::vector<long long> cnt;
+    std::vector<std::pair<int64_t, int64_t>> copy;  // LLR element range each chunk brings in
+    const int64_t cap = chunk_cap(frames, wave);
+    int64_t copied = 0;
+    for (int64_t p0 = 0, nf = 0, want = wave; p0 < frames; p0 += nf, want = std::min(2 * want, cap)) {
+      nf = (cnt.size() == 63) ? frames - p0 : chunk_frames(want, frames - p0, wave);
+      int64_t hi = 0;
+      for (int64_t p = p0; p < p0 + nf; p++) hi = std::max<int64_t>(hi, llr_offset[mem[p]] + dec->codes[code_id[mem[p]]]->h->n);
+      const int64_t lo = std::max<int64_t>(llr_offset[mem[p0]], copied);
+      copy.emplace_back(lo, std::max(hi, lo));
+      copied = std::max(copied, hi);
+      std::copy(mem.begin() + p0, mem.begin() + p0 + nf, ord.begin() + p0);
+      std::stable_sort(ord.begin() + p0, ord.begin() + p0 + nf, [&](int64_t x, int64_t y) {
+        const int rx = dec->h_rank[code_id[x]], ry = dec->h_rank[code_id[y]];
+        return rx != ry ? rx < ry : x < y;
+      });
+      cnt.push_back(nf);
+    }
+    GF2C_CUDA(cudaEventRecord(dec->pev_fork, st));
+    GF2C_CUDA(cudaStreamWaitEvent(dec->pstream, dec->pev_fork, 0));
+    GF2C_CUDA(cudaStreamWaitEvent(dec->cstream, dec->pev_fork, 0));
+    cudaStream_t cs = dec->cstream;
+    GF2C_CUDA(cudaMemcpyAsync(dec->d_order.p, ord.data(), frames * 8, cudaMemcpyHostToDevice, cs));
+    GF2C_CUDA(cudaMemcpyAsync(dec->s_cnt.p, cnt.data(), cnt.size() * 8, cudaMemcpyHostToDevice, cs));
+    GF2C_CUDA(cudaMemcpyAsync(dec->s_off1.p, llr_offset, frames * 8, cudaMemcpyHostToDevice, cs));
+    if (msg_bits) GF2C_CUDA(cudaMemcpyAsync(dec->s_off2.p, msg_offset, frames * 8, cudaMemcpyHostToDevice, cs));
+    GF2C_CUDA(cudaMemcpyAsync(dec->s_cid.p, code_id, frames * 4, cudaMemcpyHostToDevice, cs));
+    GF2C_CUDA(cudaMemcpyAsync(dec->s_mit.p, max_iter, frames * 4, cudaMemcpyHostToDevice, cs));
+    a.llr = (const float*)dec->s_llr.p;
+    a.llr_off = (const int64_t*)dec->s_off1.p;
+    a.code_id = (const int32_t*)dec->s_cid.p;
+    a.max_iter_arr = (const int32_t*)dec->s_mit.p;
+    a.msg = msg_bits ? (uint64_t*)dec->s_msg.p : nullptr;
+    a.msg_off = msg_bits ? (const int64_t*)dec->s_off2.p : nullptr;
+    a.iters = (int32_t*)dec->s_it.p;
+    a.conv = (uint8_t*)dec->s_cv.p;
+    a.synd_ok = (uint8_t*)dec->s_so.p;
+    int launches = 0;
+    for (size_t c = 0, p0 = 0; c < cnt.size(); p0 += (size_t)cnt[c], c++) {
+      const int slot = (int)(c & 1);
+      cudaStream_t s = slot ? dec->pstream : st;
+      const int64_t lo = copy[c].first, n = copy[c].second - copy[c].first;
+      if (n > 0)
+        GF2C_CUDA(cudaMemcpyAsync((float*)dec->s_llr.p + lo, llr + lo, (size_t)n * 4, cudaMemcpyHostToDevice, cs));
+      GF2C_CUDA(cudaEventRecord(dec->pev_copy[slot], cs));
+      GF2C_CUDA(cudaStreamWaitEvent(s, dec->pev_copy[slot], 0));
+      DecodeArgs b = a;
+      b.order = (const int64_t*)dec->d_order.p + p0;
+      b.frames_dev = (const long long*)dec->s_cnt.p + c;
+      if ((rc = launch_decoder(dec, b, frames, s, slot))) return rc;
+      launches++;
+    }
+    GF2C_CUDA(cudaEventRecord(dec->pev_join, dec->pstream));
+    GF2C_CUDA(cudaStreamWaitEvent(st, dec->pev_join, 0));
+    dec->last_launches = launches;
+    if (msg_bits) GF2C_CUDA(cudaMemcpyAsync(msg_bits, dec->s_msg.p, msg_total * 8, cudaMemcpyDeviceToHost, st));
+    if (iterations) GF2C_CUDA(cudaMemcpyAsync(iterations, dec->s_it.p, frames * 4, cudaMemcpyDeviceToHost, st));
+    if (converged) GF2C_CUDA(cudaMemcpyAsync(converged, dec->s_cv.p, frames, cudaMemcpyDeviceToHost, st));
+    if (syndrome_ok) GF2C_CUDA(cudaMemcpyAsync(syndrome_ok, dec->s_so.p, frames, cudaMemcpyDeviceToHost, st));
+    return check_status(dec, st);
+  }
   GF2C_CUDA(cudaMemcpyAsync(dec->s_llr.p, llr, llr_total * 4, cudaMemcpyHostToDevice, st));
   GF2C_CUDA(cudaMemcpyAsync(dec->s_off1.p, llr_offset, frames * 8, cudaMemcpyHostToDevice, st));
   if (msg_bits) GF2C_CUDA(cudaMemcpyAsync(dec->s_off2.p, msg_offset, frames * 8, cudaMemcpyHostToDevice, st));

@@ -271,11 +271,12 @@ __global__ void __launch_bounds__(512) bp_decode_kernel(const DecodeArgs a) {
   for (;;) {
     if (tid == 0) {
       const long long q = (long long)atomicAdd(a.queue, 1ull);
-      s_frame = (a.order != nullptr && q < a.frames) ? a.order[q] : q;
+      const long long nq = a.frames_dev ? *a.frames_dev : a.frames;  // queue entries
+      s_frame = (q < nq) ? (a.order != nullptr ? a.order[q] : q) : -1;
     }
     __syncthreads();
     const long long f = s_frame;
-    if (f >= a.frames) break;
+    if (f < 0 || f >= a.frames) break;
     const int cid = a.code_id ? a.code_id[f] : 0;
     if (cid < 0 || cid >= a.ncodes) {
       if (tid == 0) {

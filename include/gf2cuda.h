@@ -206,7 +206,10 @@ int gf2c_decode_batch_fallback(gf2c_decoder* primary, gf2c_decoder* fallback, co
  * decodes the frames code by code (longest codes first); a frame's results do not
  * depend on the order.  With mem ==
  * GF2C_MEM_DEVICE and use_graph = 1 the launch sequence is captured once per
- * (frames, pointers) shape into a CUDA graph and replayed. */
+ * (frames, pointers) shape into a CUDA graph and replayed.  With mem ==
+ * GF2C_MEM_HOST a large batch of several codes goes in chunks of frames in
+ * memory order (the frame order of each chunk made on the host), whose copies
+ * overlap the decoding of earlier chunks; use_graph is ignored. */
 int gf2c_decode_mixed(gf2c_decoder* dec, const float* llr, const int64_t* llr_offset,
                       const int32_t* code_id, const int32_t* max_iter, int64_t frames,
                       uint64_t* msg_bits, const int64_t* msg_offset, int32_t* iterations,

@@ -480,3 +480,46 @@ def test_layered_minsum_equals_oracle_after_unit_weight_routing(gpu, oracle):
                             msg_dtype=g.MSG_F16 if msg16 else g.MSG_F32)
         r = dec.decode_arrays(llr, 15, beliefs=True)
         assert_same_decode(r, ocode.decode(llr, 15, algo=0, sched=1, msg16=msg16), code.k())
+
+
+@pytest.mark.parametrize("kind", ["layered_sfu16", "flooding_minsum"])
+def test_mixed_host_pipeline_equals_device(gpu, kind):
+    """A mixed batch from host memory large enough for the pipelined path
+    (chunks of frames in memory order, copies on their own stream, each
+    chunk's frame order made on the host) gives the device call's results;
+    frames are laid out code by code, not in frame order."""
+    import torch
+    codes = [g.LdpcCode.dvb_t2_short(0), g.LdpcCode.dvb_t2_normal(1), g.LdpcCode.dvb_t2_short(2)]
+    kw = (dict(algorithm=g.ALGO_SPA_FAST, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16)
+          if kind == "layered_sfu16" else {})
+    dec = g.LdpcDecoder(codes[0], codes=codes, **kw)
+    rng = np.random.default_rng(12)
+    F = 2500
+    cid = rng.choice(3, F, p=[0.45, 0.1, 0.45]).astype(np.int32)
+    mit = rng.integers(5, 30, F).astype(np.int32)
+    ebn0 = [1.2, 1.1, 2.2]
+    parts, lo, base = [], np.zeros(F, np.int64), 0
+    for c in range(3):
+        idx = np.nonzero(cid == c)[0]
+        s2 = np.array([g.sigma2_from_ebn0(ebn0[c] + 0.1 * (i % 5), codes[c].rate()) for i in idx])
+        _, _, l = g.awgn_frames(codes[c], 10, c << 20, len(idx), s2, device=gpu, want_info=False, want_cw=False)
+        parts.append(l.reshape(-1))
+        lo[idx] = base + np.arange(len(idx)) * codes[c].n()
+        base += len(idx) * codes[c].n()
+    llr = torch.cat(parts)
+    assert llr.numel() * 4 >= 64 << 20
+    W = max(g.words(c.k()) for c in codes)
+    mo = np.arange(F, dtype=np.int64) * W
+    d = dict(msg=torch.zeros(F * W, dtype=torch.int64, device=gpu), iters=torch.zeros(F, dtype=torch.int32, device=gpu),
+             conv=torch.zeros(F, dtype=torch.uint8, device=gpu), so=torch.zeros(F, dtype=torch.uint8, device=gpu))
+    dt = lambda x: torch.from_numpy(x).to(gpu)
+    dec.decode_mixed_tensors(llr, dt(lo), dt(cid), dt(mit), d["msg"], dt(mo), d["iters"], d["conv"], d["so"],
+                             use_graph=False)
+    torch.cuda.synchronize()
+    h = dec.decode_mixed_arrays(llr.cpu().numpy(), lo, cid, mit, mo)
+    assert dec.last_launches() > 2  # several chunks
+    assert (h["iters"] == d["iters"].cpu().numpy()).all()
+    assert (h["conv"] == d["conv"].cpu().numpy().astype(bool)).all()
+    assert (h["synd_ok"] == d["so"].cpu().numpy().astype(bool)).all()
+    hm = h["msg"].view(np.int64)
+    assert (hm == d["msg"].cpu().numpy()[:hm.size]).all()
