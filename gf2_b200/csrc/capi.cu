@@ -415,7 +415,10 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
     }
   }
   const size_t msg_bytes = o.msg_dtype == GF2C_MSG_F16 ? 2 : 4;
-  const long long c2v_bytes = (((long long)d->max_e_slots * msg_bytes) + 255) / 256 * 256;
+  // per-edge messages, or (layered min-sum family) one compressed state per check
+  const long long c2v_bytes = (std::max((long long)d->max_e_slots * (long long)msg_bytes,
+                                        (long long)d->max_m * (o.msg_dtype == GF2C_MSG_F16 ? 8 : 16)) +
+                               255) / 256 * 256;
   d->app_offset = c2v_bytes;
   const bool need_gapp = d->max_n > d->smem_app_floats;
   d->work_stride = c2v_bytes + (need_gapp ? ((long long)d->max_n * 4 + 255) / 256 * 256 : 0);
@@ -493,12 +496,15 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   if (layered && d->codes.size() == 1 && o.algorithm != GF2C_ALGO_SPA && threads <= 384 &&
       !std::getenv("GF2C_NO_STAGE")) {
     const HostCode& h = *d->codes[0]->h;
-    bool ok = h.cg.size() >= 3;
+    // the min-sum family keeps compressed check states and stages nothing (the
+    // staged kernel then only needs its two mbarriers)
+    const bool states = layered_state_mode(o.algorithm, d->dcmax, true);
+    bool ok = states || h.cg.size() >= 3;
     size_t mx = 0;
     for (const int4& G : h.cg) {
       const size_t off = (size_t)G.w * msg_bytes, by = (size_t)G.z * G.y * msg_bytes;
-      ok = ok && off % 16 == 0 && by % 16 == 0;
-      mx = std::max(mx, by);
+      ok = ok && (states || (off % 16 == 0 && by % 16 == 0));
+      if (!states) mx = std::max(mx, by);
     }
     const void* k = ok ? layered_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax, threads, true, o.blocks_per_sm)
                        : nullptr;

@@ -227,6 +227,13 @@ int layered_dcmax_bucket(int max_dc);
 // bps: requested CTAs per SM (0 = any); 192 threads with 5 or more picks the 64-register build
 const void* layered_kernel_ptr(int algo, int msg16, int dcmax, int maxt, bool stage = false, int bps = 0);
 size_t layered_smem_bytes(int smem_app_floats, int bitmap_words);
+// Layered min-sum / normalised-offset min-sum on the single-code (staged)
+// kernels with the fused row paths: one compressed state per check (8 bytes
+// for binary16 messages, 16 for FP32) replaces the per-edge messages, and
+// nothing is staged in shared memory.
+__host__ __device__ constexpr bool layered_state_mode(int algo, int dcmax, bool staged) {
+  return (algo == GF2C_ALGO_MINSUM || algo == GF2C_ALGO_NMS) && staged && dcmax > 0 && dcmax <= 22;
+}
 size_t decode_smem_bytes(int smem_app_floats, int bitmap_words);
 
 int launch_nms_forward(const DevCode* dcode, const DevCode& h, int T, int L, const float* llr, const uint64_t* cw,

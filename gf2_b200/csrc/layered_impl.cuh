@@ -113,6 +113,44 @@ struct SharedOld {
   }
 };
 
+// Min-sum family (min-sum, normalised / offset min-sum): every message a check
+// sends is +-r1 or +-r2 (the two magnitudes rounded through the message type),
+// r2 on slot i1 only, so a check keeps one compressed state instead of one
+// message per edge: binary16 messages {r1 | r2 << 16, sign bits | i1 << 24}
+// (8 bytes, up to 22 slots), FP32 messages {r1, r2, sign bits, i1} (16
+// bytes).  Bit i of the sign bits flips slot i's message.  The messages it
+// gives back are bit-identical to the per-edge ones.
+struct StateOld {
+  float r1, r2;
+  uint32_t sig;
+  int i1;
+  __device__ __forceinline__ float ld(int i) const {
+    return __uint_as_float(__float_as_uint(i == i1 ? r2 : r1) ^ (((sig >> i) & 1u) << 31));
+  }
+};
+template <int MSG16>
+__device__ __forceinline__ StateOld load_state(const void* cst, int ci) {
+  if constexpr (MSG16) {
+    const uint2 v = __ldcs((const uint2*)cst + ci);
+    return StateOld{__half2float(__ushort_as_half((unsigned short)(v.x & 0xffffu))),
+                    __half2float(__ushort_as_half((unsigned short)(v.x >> 16))), v.y & 0xffffffu,
+                    (int)(v.y >> 24) == 31 ? -1 : (int)(v.y >> 24)};
+  } else {
+    const uint4 v = __ldcs((const uint4*)cst + ci);
+    return StateOld{__uint_as_float(v.x), __uint_as_float(v.y), v.z, (int)v.w};
+  }
+}
+// r1, r2 already rounded through the message type; i1 = -1: no slot takes r2
+template <int MSG16>
+__device__ __forceinline__ void store_state(void* cst, int ci, float r1, float r2, uint32_t sig, int i1) {
+  if constexpr (MSG16) {
+    const uint32_t h1 = __half_as_ushort(__float2half_rn(r1)), h2 = __half_as_ushort(__float2half_rn(r2));
+    __stcs((uint2*)cst + ci, make_uint2(h1 | (h2 << 16), sig | ((uint32_t)(i1 & 31) << 24)));
+  } else {
+    __stcs((uint4*)cst + ci, make_uint4(__float_as_uint(r1), __float_as_uint(r2), sig, (uint32_t)i1));
+  }
+}
+
 // TMA (bulk copy engine) helpers: a 1-D global -> shared copy whose bytes an
 // mbarrier counts, and bounded waits on the mbarrier's phase.
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
@@ -356,11 +394,11 @@ __device__ __forceinline__ void spa_fast_rep_b(const int2* __restrict__ sd, int 
 // message rounded through the message type, APP + (c2v_new - c2v_old)), so
 // results are bit-identical.  PART: the row group has d < D slots; slots
 // d..D-1 are absent (no load, no store).
-template <int ALGO, int MSG16, int D, bool PART, class OM>
+template <int ALGO, int MSG16, int D, bool PART, class OM, bool ST = false>
 __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
                                        typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om, bool first,
                                        float al, float be,
-                                       const LayerSmem& S, int d) {
+                                       const LayerSmem& S, int d, int ci = 0) {
   typedef MsgIO<MSG16> IO;
   float ap[D], o[D];
 #pragma unroll
@@ -398,7 +436,9 @@ __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int n
     if (PART && i >= d) continue;
     const uint32_t sflip = ((neg >> i) ^ negp) & 1u;
     const float out = __uint_as_float(__float_as_uint((i == i1) ? r2 : r1) ^ (sflip << 31));
-    if constexpr (MSG16) {
+    if constexpr (ST) {
+      // one compressed state per check, stored after the loop
+    } else if constexpr (MSG16) {
       const uint32_t h = (i == i1) ? __half_as_ushort(__float2half_rn(r2)) : __half_as_ushort(__float2half_rn(r1));
       __stcs((unsigned short*)c2v + s0 + i * nchk, (unsigned short)(h ^ (sflip << 15)));
     } else {
@@ -407,6 +447,10 @@ __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int n
     const float nw = __fadd_rn(ap[i], __fsub_rn(out, o[i]));
     app[slot_u(__ldg(&sd[i]), t, nchk)] = nw;
     flips |= (uint32_t)(((apneg >> i) & 1u) != (uint32_t)(nw < 0.0f)) << i;
+  }
+  if constexpr (ST) {
+    const uint32_t real = PART ? ((1u << d) - 1u) : (uint32_t)((1ull << D) - 1ull);
+    store_state<MSG16>(c2v, ci, r1, r2, (neg ^ (0u - negp)) & real, i1);
   }
   while (flips) {  // rare after the first iterations
     const int i = __ffs(flips) - 1;
@@ -421,11 +465,11 @@ __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int n
 // B (spa_fast_rep_b, after one barrier), the other slots update their unique
 // variable now.  Same additions in the same order as the slot-by-slot general
 // path, so results are bit-identical.
-template <int ALGO, int MSG16, int D, bool PART, class OM>
+template <int ALGO, int MSG16, int D, bool PART, class OM, bool ST = false>
 __device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
                                          typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om, bool first,
                                          float al, float be,
-                                         uint32_t sync, float* dbuf, const LayerSmem& S, int d) {
+                                         uint32_t sync, float* dbuf, const LayerSmem& S, int d, int ci = 0) {
   typedef MsgIO<MSG16> IO;
   const uint32_t rep = sync | (sync << 1);  // slots inside a run
   float ap[D], o[D];
@@ -462,7 +506,7 @@ __device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int
     if (PART && i >= d) continue;
     const float mag = (i == i1) ? mag2 : mag1;
     const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
-    st_msg<MSG16>(c2v, s0 + i * nchk, out);
+    if constexpr (!ST) st_msg<MSG16>(c2v, s0 + i * nchk, out);
     const float delta = __fsub_rn(out, o[i]);
     if ((rep >> i) & 1u) {
       dbuf[i * nchk + t] = delta;
@@ -471,6 +515,10 @@ __device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int
       app_put(app, v, ap[i] < 0.0f, __fadd_rn(ap[i], delta), S);
     }
   }
+  if constexpr (ST) {
+    const uint32_t real = PART ? ((1u << d) - 1u) : (uint32_t)((1ull << D) - 1ull);
+    store_state<MSG16>(c2v, ci, IO::rt(mag1), IO::rt(mag2), (neg ^ (0u - negp)) & real, i1);
+  }
 }
 
 // General check update (any algorithm, absent slots, repeated variables):
@@ -478,13 +526,15 @@ __device__ __forceinline__ void ms_rep_a(const int2* __restrict__ sd, int t, int
 // `direct` (a row group without repeated variables) the posteriors are
 // updated here; otherwise the deltas to add (slot order) are returned in wd[]
 // with the slot's variable in vd[] (-1: no edge).
-template <int ALGO, int MSG16, int DCMAX, class OM>
+template <int ALGO, int MSG16, int DCMAX, class OM, bool ST = false>
 __device__ __forceinline__ void general_row(const DecodeArgs& a, const int2* __restrict__ sd, int t, int nchk, int s0,
                                             float* app, typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om,
                                             bool first, int d, uint32_t ab, bool direct, float al, float be,
                                             const LayerSmem& S, float (&wd)[DCMAX],
-                                            int (&vv)[DCMAX]) {
+                                            int (&vv)[DCMAX], int ci = 0) {
   typedef MsgIO<MSG16> IO;
+  float smag1 = 0.0f, smag2 = 0.0f;  // min-sum family: the check's two magnitudes and argmin
+  int si1 = -1;
   float ap[DCMAX], o[DCMAX], w[DCMAX];
   uint32_t real = 0, neg = 0, apneg = 0;
 #pragma unroll
@@ -528,6 +578,9 @@ __device__ __forceinline__ void general_row(const DecodeArgs& a, const int2* __r
       mag1 = __fmul_rn(al, d1 > 0.0f ? d1 : 0.0f);
       mag2 = __fmul_rn(al, d2 > 0.0f ? d2 : 0.0f);
     }
+    smag1 = mag1;
+    smag2 = mag2;
+    si1 = i1;
 #pragma unroll
     for (int i = 0; i < DCMAX; i++) {
       const float mag = (i == i1) ? mag2 : mag1;
@@ -576,7 +629,7 @@ __device__ __forceinline__ void general_row(const DecodeArgs& a, const int2* __r
     wd[i] = 0.0f;
     if ((real >> i) & 1u) {
       const float out = IO::rt(w[i]);
-      st_msg<MSG16>(c2v, s0 + i * nchk, out);
+      if constexpr (!ST) st_msg<MSG16>(c2v, s0 + i * nchk, out);
       if (ALGO == L_SPA_FAST) {
         if (direct) app_put(app, vv[i], (apneg >> i) & 1u, ap[i] + out, S);
         else wd[i] = out - o[i];
@@ -587,6 +640,7 @@ __device__ __forceinline__ void general_row(const DecodeArgs& a, const int2* __r
       }
     }
   }
+  if constexpr (ST) store_state<MSG16>(c2v, ci, IO::rt(smag1), IO::rt(smag2), (neg ^ (0u - (uint32_t)negp)) & real, si1);
 }
 
 // Iterations of one frame with row groups of at most DCMAX slots; returns the
@@ -621,6 +675,10 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
   // fused row paths: every algorithm but the exact sum-product
   constexpr bool kFused = (ALGO == L_SPA_FAST || ALGO == L_MS || ALGO == L_NMS) && DCMAX <= 22;
   constexpr int kMsgBytes = MSG16 ? 2 : 4;
+  // the min-sum family on the single-code (staged) kernels keeps one compressed
+  // state per check (flattened check index) instead of per-edge messages, read
+  // and written by the check's thread; nothing is staged
+  constexpr bool ST = layered_state_mode(ALGO, DCMAX, STG);
   for (;;) {
     const int tw = (a.nms_iters > 0) ? min(it, a.nms_iters - 1) : 0;
     const bool first = (it == 0);
@@ -632,9 +690,13 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
       const int t = act ? tid : 0;
       const int s0 = G.w + t;
       const int2* __restrict__ sd = sdesc + spcg[g].w;
-      typedef typename std::conditional<STG, SharedOld<MSG16>, GlobalOld<MSG16>>::type OM;
+      const int c0 = spcg[g].x;  // flattened index of the row group's first check
+      typedef typename std::conditional<
+          ST, StateOld, typename std::conditional<STG, SharedOld<MSG16>, GlobalOld<MSG16>>::type>::type OM;
       OM om;
-      if constexpr (STG) {
+      if constexpr (ST) {
+        om = (act && !first) ? load_state<MSG16>(c2v, c0 + t) : StateOld{};
+      } else if constexpr (STG) {
         const uint32_t b = stg.step & 1u;
         if (!first) {  // this row group's old messages: wait for the copy into buffer b
           if (!mbar_wait_bounded(stg.bar + 8 * b, (stg.phase >> b) & 1u)) {
@@ -673,7 +735,9 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
       }
       // old-message reader of check tc of this row group
       auto old_of = [&](int tc) -> OM {
-        if constexpr (STG)
+        if constexpr (ST)
+          return first ? StateOld{} : load_state<MSG16>(c2v, c0 + tc);
+        else if constexpr (STG)
           return OM{om.a + (uint32_t)((tc - t) * kMsgBytes), om.stride};
         else
           return OM{c2v + G.w + tc, nchk};
@@ -689,9 +753,11 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
               spa_fast_rep_a<MSG16, DCMAX, true>(sd, tc, nchk, sc, app, c2v, omc, first, sync, S.dbuf, S, d);
           } else if constexpr (kFused) {
             if (d == DCMAX)
-              ms_rep_a<ALGO, MSG16, DCMAX, false>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, sync, S.dbuf, S, d);
+              ms_rep_a<ALGO, MSG16, DCMAX, false, OM, ST>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, sync, S.dbuf, S,
+                                                     d, c0 + tc);
             else
-              ms_rep_a<ALGO, MSG16, DCMAX, true>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, sync, S.dbuf, S, d);
+              ms_rep_a<ALGO, MSG16, DCMAX, true, OM, ST>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, sync, S.dbuf, S,
+                                                    d, c0 + tc);
           }
         }
         __syncthreads();
@@ -709,14 +775,17 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
                 spa_fast_row<MSG16, DCMAX, true>(sd, tc, nchk, sc, app, c2v, omc, first, S, d);
             } else if constexpr (kFused) {
               if (d == DCMAX)
-                ms_row<ALGO, MSG16, DCMAX, false>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, S, d);
+                ms_row<ALGO, MSG16, DCMAX, false, OM, ST>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, S, d,
+                                                          c0 + tc);
               else
-                ms_row<ALGO, MSG16, DCMAX, true>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, S, d);
+                ms_row<ALGO, MSG16, DCMAX, true, OM, ST>(sd, tc, nchk, sc, app, c2v, omc, first, al, be, S, d,
+                                                         c0 + tc);
             }
           } else {
             float wd[DCMAX];
             int vd[DCMAX];
-            general_row<ALGO, MSG16, DCMAX>(a, sd, tc, nchk, sc, app, c2v, omc, first, d, ab, true, al, be, S, wd, vd);
+            general_row<ALGO, MSG16, DCMAX, OM, ST>(a, sd, tc, nchk, sc, app, c2v, omc, first, d, ab, true, al, be, S, wd,
+                                                   vd, c0 + tc);
           }
         }
       } else if (!MULTI || NT >= nchk) {
@@ -726,7 +795,8 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
         int vd[DCMAX];
         if (act) {
           const uint32_t ab = (t == 0) ? __ldg(&absent[g]) : 0u;
-          general_row<ALGO, MSG16, DCMAX>(a, sd, t, nchk, s0, app, c2v, om, first, d, ab, false, al, be, S, wd, vd);
+          general_row<ALGO, MSG16, DCMAX, OM, ST>(a, sd, t, nchk, s0, app, c2v, om, first, d, ab, false, al, be, S, wd, vd,
+                                                 c0 + t);
         }
         __syncthreads();  // all pre-layer APP reads done
 #pragma unroll
@@ -748,8 +818,8 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
           float wd[DCMAX];
           int vd[DCMAX];
           const uint32_t ab = (tc == 0) ? __ldg(&absent[g]) : 0u;
-          general_row<ALGO, MSG16, DCMAX>(a, sd, tc, nchk, G.w + tc, app, c2v, old_of(tc), first, d, ab, false, al, be,
-                                         S, wd, vd);
+          general_row<ALGO, MSG16, DCMAX, OM, ST>(a, sd, tc, nchk, G.w + tc, app, c2v, old_of(tc), first, d, ab, false,
+                                                 al, be, S, wd, vd, c0 + tc);
 #pragma unroll
           for (int i = 0; i < DCMAX; i++)
             if (i < d && vd[i] >= 0) S.dbuf[i * nchk + tc] = wd[i];
@@ -766,9 +836,9 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
           if ((sync >> i) & 1u) __syncthreads();
         }
       }
-      if constexpr (STG) fence_proxy_async_global();  // this thread's message stores before later TMA reads
+      if constexpr (STG && !ST) fence_proxy_async_global();  // this thread's message stores before later TMA reads
       __syncthreads();
-      if constexpr (STG) {
+      if constexpr (STG && !ST) {
         stg.step++;
         if (*abort) return;
       }
