@@ -523,3 +523,28 @@ def test_mixed_host_pipeline_equals_device(gpu, kind):
     assert (h["synd_ok"] == d["so"].cpu().numpy().astype(bool)).all()
     hm = h["msg"].view(np.int64)
     assert (hm == d["msg"].cpu().numpy()[:hm.size]).all()
+
+
+@pytest.mark.parametrize("idx,msg", [(1, g.MSG_F16), (1, g.MSG_F32), (6, g.MSG_F16), (5, g.MSG_F16), (5, g.MSG_F32)])
+def test_layered_compressed_states_equal_per_edge_messages(gpu, monkeypatch, idx, msg):
+    """The single-code min-sum family kernels keep one compressed state per
+    check; with staging disabled the decoder runs the per-edge-message kernel.
+    Both give bit-identical results (normal 3/5 and 5/6: repeated-variable row
+    groups; short 1/2: posteriors in shared memory; FP16 and FP32 messages)."""
+    import torch
+    code = dvb(idx)
+    L = code.layers()
+    rng = np.random.default_rng(30 + idx)
+    kw = dict(algorithm=g.ALGO_NMS, schedule=g.SCHED_LAYERED, msg_dtype=msg,
+              nms_alpha=(0.7 + 0.3 * rng.random((6, L))).astype(np.float32),
+              nms_beta=(0.3 * rng.random((6, L))).astype(np.float32))
+    ebn0 = {1: 1.3, 6: 1.4, 5: 3.3}[idx]
+    _, _, llr = g.awgn_frames(code, 19, 0, 300, g.sigma2_from_ebn0(ebn0, code.rate()), device=gpu,
+                              want_info=False, want_cw=False)
+    states = g.LdpcDecoder(code, **kw).decode_tensors(llr, 25, beliefs=True)
+    monkeypatch.setenv("GF2C_NO_STAGE", "1")
+    per_edge = g.LdpcDecoder(code, **kw).decode_tensors(llr, 25, beliefs=True)
+    torch.cuda.synchronize()
+    for key in ("msg", "iters", "conv", "synd_ok"):
+        assert torch.equal(states[key], per_edge[key]), key
+    assert torch.equal(states["beliefs"].view(torch.int32), per_edge["beliefs"].view(torch.int32))
