@@ -277,16 +277,14 @@ class SingleCode:
         _, _, self.llr = g.awgn_frames(self.code, 1, rank * self.frames, self.frames, s2, device=dev,
                                        want_info=False, want_cw=False)
         msg = g.MSG_F16 if w["msg16"] else g.MSG_F32
-        shape = (0, 0)
-        if w["sched"] == g.SCHED_LAYERED:
-            from gf2_b200 import autotune
-            sample = self.llr[:min(2048, self.frames)]
-            shape, _ = autotune.tune([self.code], w["algo"], w["sched"], msg,
-                                     lambda d: d.decode_tensors(sample, w["max_iter"]))
+        from gf2_b200 import autotune
+        sample = self.llr[:min(2048, self.frames)]
+        shape, _ = autotune.tune([self.code], w["algo"], w["sched"], msg,
+                                 lambda d: d.decode_tensors(sample, w["max_iter"]))
         self.dec = g.LdpcDecoder(self.code, algorithm=w["algo"], schedule=w["sched"], msg_dtype=msg,
                                  threads_per_block=shape[0], blocks_per_sm=shape[1])
         self.out = None
-        self.desc = w["desc"] + (f", autotuned launch shape {tuple(shape)}" if w["sched"] == g.SCHED_LAYERED else "")
+        self.desc = w["desc"] + f", autotuned launch shape {tuple(shape)}"
         self.dtype = "f16 storage / f32 math" if w["msg16"] else "f32"
         self.msg_bytes = 2 if w["msg16"] else 4
 

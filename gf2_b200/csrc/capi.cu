@@ -423,7 +423,7 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   const bool need_gapp = d->max_n > d->smem_app_floats;
   d->work_stride = c2v_bytes + (need_gapp ? ((long long)d->max_n * 4 + 255) / 256 * 256 : 0);
   d->kernel = layered ? layered_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax, threads)
-                      : flood_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax);
+                      : flood_kernel_ptr(o.algorithm, o.msg_dtype, d->dcmax, threads);
   if (layered && threads <= 384) {
     // codes of different slot counts (a mixed batch): the kernel that runs each
     // frame with its own code's exact slot count, where one exists
@@ -467,9 +467,10 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
     d->threads = threads;
     d->state_flood = true;
   }
+  if (!layered && !d->state_flood && threads > 512 && !d->kernel)
+    return set_error(GF2C_ERR_INVALID_ARG,
+                     "flooding schedule: threads_per_block above 512 needs a code of check degree <= 8");
   if (!d->kernel && !multi) return set_error(GF2C_ERR_UNSUPPORTED, "no decode kernel for this configuration");
-  if (!layered && !d->state_flood && threads > 512)
-    return set_error(GF2C_ERR_INVALID_ARG, "flooding schedule: threads_per_block must be <= 512");
   if (multi && d->lay_dbuf_floats > 0) {
     // several checks per thread: the delta buffer is required
     d->smem = (size_t)d->lay_dbuf_off + (size_t)d->lay_dbuf_floats * 4;

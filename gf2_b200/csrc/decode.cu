@@ -254,8 +254,8 @@ __device__ __forceinline__ int syndrome_any(const FrameCtx& F, const uint32_t* b
   return __syncthreads_or(par);
 }
 
-template <int ALGO, int MSG16, int DCMAX>
-__global__ void __launch_bounds__(512) bp_decode_kernel(const DecodeArgs a) {
+template <int ALGO, int MSG16, int DCMAX, int MAXT = 512>
+__global__ void __launch_bounds__(MAXT) bp_decode_kernel(const DecodeArgs a) {
   typedef MsgIO<MSG16> IO;
   typedef typename IO::T MsgT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -400,7 +400,10 @@ size_t decode_smem_bytes(int smem_app_floats, int bitmap_words) {
 }
 
 template <int ALGO, int MSG16>
-static const void* kernel_dc(int dcmax) {
+static const void* kernel_dc(int dcmax, int threads) {
+  // up to 1024 threads per frame for checks of at most 8 slots (64 registers
+  // suffice; short batches, where a frame's latency sets the step, gain)
+  if (threads > 512) return dcmax == 8 ? (const void*)bp_decode_kernel<ALGO, MSG16, 8, 1024> : nullptr;
   switch (dcmax) {
     case 8: return (const void*)bp_decode_kernel<ALGO, MSG16, 8>;
     case 16: return (const void*)bp_decode_kernel<ALGO, MSG16, 16>;
@@ -549,13 +552,15 @@ cudaError_t launch_key_order(const float* llr, int n, int64_t frames, float* key
   return cudaGetLastError();
 }
 
-// Flooding-schedule kernel for (algorithm, message type, degree bucket).
-const void* flood_kernel_ptr(int algo, int msg16, int dcmax) {
+// Flooding-schedule kernel for (algorithm, message type, degree bucket,
+// threads per block); nullptr where none exists.
+const void* flood_kernel_ptr(int algo, int msg16, int dcmax, int threads) {
   switch (algo) {
-    case ALGO_MS: return msg16 ? kernel_dc<ALGO_MS, 1>(dcmax) : kernel_dc<ALGO_MS, 0>(dcmax);
-    case ALGO_SPA: return msg16 ? kernel_dc<ALGO_SPA, 1>(dcmax) : kernel_dc<ALGO_SPA, 0>(dcmax);
-    case ALGO_NMS: return msg16 ? kernel_dc<ALGO_NMS, 1>(dcmax) : kernel_dc<ALGO_NMS, 0>(dcmax);
-    case ALGO_SPA_FAST: return msg16 ? kernel_dc<ALGO_SPA_FAST, 1>(dcmax) : kernel_dc<ALGO_SPA_FAST, 0>(dcmax);
+    case ALGO_MS: return msg16 ? kernel_dc<ALGO_MS, 1>(dcmax, threads) : kernel_dc<ALGO_MS, 0>(dcmax, threads);
+    case ALGO_SPA: return msg16 ? kernel_dc<ALGO_SPA, 1>(dcmax, threads) : kernel_dc<ALGO_SPA, 0>(dcmax, threads);
+    case ALGO_NMS: return msg16 ? kernel_dc<ALGO_NMS, 1>(dcmax, threads) : kernel_dc<ALGO_NMS, 0>(dcmax, threads);
+    case ALGO_SPA_FAST:
+      return msg16 ? kernel_dc<ALGO_SPA_FAST, 1>(dcmax, threads) : kernel_dc<ALGO_SPA_FAST, 0>(dcmax, threads);
   }
   return nullptr;
 }

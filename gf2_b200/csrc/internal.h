@@ -206,7 +206,7 @@ struct DecodeArgs {
   long long sf_llr_off, sf_st_off, sf_app_off;
 };
 
-const void* flood_kernel_ptr(int algo, int msg16, int dcmax);
+const void* flood_kernel_ptr(int algo, int msg16, int dcmax, int threads = 512);
 // Frame order of a mixed batch (one CTA): frames grouped by rank_of[code id],
 // ascending rank, ids outside [0, ncodes) last; ascending frame index within a group.
 cudaError_t launch_mixed_order(const int32_t* code_id, int64_t frames, const int32_t* rank_of, int ncodes,
