@@ -21,6 +21,13 @@
 // always-valid addresses before any arithmetic (memory-level parallelism), and
 // then the check node, the message stores and the APP updates follow.
 //
+// Old messages: the sum-product rules keep one message per edge, a row
+// group's messages one contiguous block that a TMA copy stages in shared
+// memory while the previous row group is decoded; the min-sum family keeps one
+// compressed state per check instead (its two magnitudes, sign bits, argmin),
+// read and written by the check's own thread, and one warp has the copy engine
+// prefetch into L2 the variable groups (and states) of the next row group.
+//
 // A row group whose variables are all distinct writes the new APP directly
 // from the thread that read it (one barrier per row group); a row group with
 // repeated variables (DVB-T2 blocks holding several circulants) applies its
@@ -191,6 +198,13 @@ __device__ __forceinline__ void tma_load_1d(uint32_t dst, const void* src, uint3
 }
 __device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+// Bulk prefetch of [p, p + bytes) into L2 (no shared memory, no completion to
+// wait for); the range is widened to 16-byte boundaries.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  const uintptr_t a = (uintptr_t)p & ~(uintptr_t)15;
+  const uint32_t n = (uint32_t)(((uintptr_t)p + bytes - a + 15) & ~(uintptr_t)15);
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(n) : "memory");
+}
 
 // Shared-memory message stage of the layered kernel: two buffers of one row
 // group's messages each (the row group being decoded and the next one, whose
@@ -679,6 +693,7 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
   // state per check (flattened check index) instead of per-edge messages, read
   // and written by the check's thread; nothing is staged
   constexpr bool ST = layered_state_mode(ALGO, DCMAX, STG);
+  const bool pf = __isGlobal(app);  // posteriors in the workspace (not on chip)
   for (;;) {
     const int tw = (a.nms_iters > 0) ? min(it, a.nms_iters - 1) : 0;
     const bool first = (it == 0);
@@ -722,6 +737,25 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
         om = OM{stg.buf + b * stg.bytes + (uint32_t)(t * kMsgBytes), (uint32_t)(nchk * kMsgBytes)};
       } else {
         om = OM{c2v + s0, nchk};
+      }
+      // Posteriors in the workspace and no message stage running on the copy
+      // engine: the next row group's slots each read one whole variable group
+      // (Z consecutive posteriors); lane i of the last warp has slot i's group
+      // (lane 31: the compressed states of the row group) prefetched into L2,
+      // so that those gathers wait on L2 rather than DRAM.  (Issued by one
+      // thread in a loop, or next to the sum-product stage copies, it was slower.)
+      if constexpr (!STG || ST) {
+        if (pf && (tid >> 5) == ((int)blockDim.x >> 5) - 1) {  // lane i of the last warp: slot i
+          const int lane = tid & 31;
+          const int gn = (g + 1 < ncg) ? g + 1 : 0;
+          const int4 Gn = spcg[gn];
+          if (lane < Gn.z) {
+            const int2 D = __ldg(&sdesc[Gn.w + lane]);
+            prefetch_l2(app + (D.x + D.y - Gn.y), (uint32_t)Gn.y * 4u);
+          } else if (ST && lane == 31) {
+            prefetch_l2((const char*)c2v + (size_t)Gn.x * (MSG16 ? 8 : 16), (uint32_t)Gn.y * (MSG16 ? 8u : 16u));
+          }
+        }
       }
       // row group with repeated variables, all slots real everywhere: one barrier
       // (fewer slots than DCMAX: the PART variants)
