@@ -109,6 +109,21 @@ static int decode() {
   for (size_t i = 0; i < s.n(); i++) l[i] = Llr(c.get(i) ? -4.0f : 4.0f);
   r = ds.decode_iterative(l, 20);
   EXPECT(r.converged && r.decoded_bits == msg);
+  // a decoder with a layered fallback: one primary iteration leaves the noisy
+  // frame failing, the fallback finishes it; the clean frame stays with the
+  // primary decoder
+  {
+    gf2c_decoder_opts lo;
+    gf2c_decoder_opts_default(&lo);
+    lo.schedule = GF2C_SCHED_LAYERED;
+    gf2::LdpcDecoder prim(s, &lo), fb(s, &lo);
+    std::vector<Llr> noisy = l;
+    for (size_t i = 0; i < s.n(); i += 7) noisy[i] = Llr(-0.25f * noisy[i].value());
+    size_t redecoded = 0;
+    auto rf = prim.decode_many_with_fallback(fb, {l, noisy}, 1, 30, &redecoded);
+    EXPECT(rf.size() == 2 && rf[0].decoded_bits == msg && rf[0].iterations == 1);
+    EXPECT(redecoded == 1 && rf[1].syndrome_check_passed && rf[1].decoded_bits == msg && rf[1].iterations > 1);
+  }
   // outer BCH: t errors corrected (bch/dvb_t2/mod.rs roundtrip tests)
   auto bch = gf2::BchCode::dvb_t2(1, gf2::CodeRate::Rate1_2);
   gf2::BitVec bm = gf2::BitVec::zeros(bch.k());

@@ -211,17 +211,50 @@ class LdpcDecoder {
   }
 
   std::vector<DecoderResult> decode_many(const std::vector<std::vector<Llr>>& blocks, size_t max_iterations) {
-    const size_t F = blocks.size(), N = n(), K = k(), W = (K + 63) / 64;
-    std::vector<float> llr(F * N);
-    for (size_t f = 0; f < F; f++) {
-      if (blocks[f].size() != N) throw std::invalid_argument("LLR length must equal n");
-      for (size_t i = 0; i < N; i++) llr[f * N + i] = blocks[f][i].value();
-    }
+    const size_t F = blocks.size(), K = k(), W = (K + 63) / 64;
+    std::vector<float> llr = flatten(blocks);
     std::vector<uint64_t> msg(F * W);
     std::vector<int32_t> it(F);
     std::vector<uint8_t> cv(F), so(F);
     check(gf2c_decode_batch(h_.get(), llr.data(), (int64_t)F, (int32_t)max_iterations, msg.data(), it.data(),
                             cv.data(), so.data(), nullptr, GF2C_MEM_HOST, nullptr));
+    return results(F, msg, it, cv, so);
+  }
+
+  // This decoder on every frame, then `fallback` (a layered decoder of the
+  // same code) on the frames whose syndrome still fails; no counterpart in the
+  // reference.  *redecoded (optional): frames the fallback decoded again.
+  std::vector<DecoderResult> decode_many_with_fallback(LdpcDecoder& fallback,
+                                                       const std::vector<std::vector<Llr>>& blocks,
+                                                       size_t max_iterations, size_t fallback_iterations,
+                                                       size_t* redecoded = nullptr) {
+    const size_t F = blocks.size(), K = k(), W = (K + 63) / 64;
+    if (F == 0) return {};
+    std::vector<float> llr = flatten(blocks);
+    std::vector<uint64_t> msg(F * W);
+    std::vector<int32_t> it(F);
+    std::vector<uint8_t> cv(F), so(F);
+    int64_t count = 0;
+    check(gf2c_decode_batch_fallback(h_.get(), fallback.h_.get(), llr.data(), (int64_t)F, (int32_t)max_iterations,
+                                     (int32_t)fallback_iterations, msg.data(), it.data(), cv.data(), so.data(), &count,
+                                     GF2C_MEM_HOST, nullptr));
+    if (redecoded) *redecoded = (size_t)count;
+    return results(F, msg, it, cv, so);
+  }
+
+ private:
+  std::vector<float> flatten(const std::vector<std::vector<Llr>>& blocks) const {
+    const size_t F = blocks.size(), N = n();
+    std::vector<float> llr(F * N);
+    for (size_t f = 0; f < F; f++) {
+      if (blocks[f].size() != N) throw std::invalid_argument("LLR length must equal n");
+      for (size_t i = 0; i < N; i++) llr[f * N + i] = blocks[f][i].value();
+    }
+    return llr;
+  }
+  std::vector<DecoderResult> results(size_t F, const std::vector<uint64_t>& msg, const std::vector<int32_t>& it,
+                                     const std::vector<uint8_t>& cv, const std::vector<uint8_t>& so) const {
+    const size_t K = k(), W = (K + 63) / 64;
     std::vector<DecoderResult> out(F);
     for (size_t f = 0; f < F; f++) {
       BitVec b = BitVec::zeros(K);
@@ -230,8 +263,6 @@ class LdpcDecoder {
     }
     return out;
   }
-
- private:
   LdpcCode code_;
   std::shared_ptr<gf2c_decoder> h_;
   size_t last_ = 0;
