@@ -512,9 +512,13 @@ class LdpcDecoder:
                            iters=torch.zeros(F, dtype=torch.int32, pin_memory=pin),
                            conv=torch.zeros(F, dtype=torch.uint8, pin_memory=pin),
                            synd_ok=torch.zeros(F, dtype=torch.uint8, pin_memory=pin))
-            for k in ("msg", "iters", "conv", "synd_ok"):
-                if out[k].is_cuda or not out[k].is_contiguous() or out[k].shape[0] != F:
-                    raise ValueError("host outputs must be contiguous CPU tensors of the batch's frames")
+            want = dict(msg=torch.int64, iters=torch.int32, conv=torch.uint8, synd_ok=torch.uint8)
+            for k, dt in want.items():
+                if out[k].is_cuda or not out[k].is_contiguous() or out[k].shape[0] != F or out[k].dtype != dt:
+                    raise ValueError("host outputs must be contiguous CPU tensors of the batch's frames "
+                                     "(msg int64 [F, words(k)], iters int32, conv / synd_ok uint8)")
+            if out["msg"].dim() != 2 or out["msg"].shape[1] != words(self.k()):
+                raise ValueError("msg must be int64 [frames, words(k)]")
             cnt = np.zeros(1, np.int64)
             C.check(C.lib.gf2c_decode_batch_fallback(self._h, fallback._h, _ptr(llr), F, int(max_iterations),
                                                      int(fallback_iterations), _ptr(out["msg"]), _ptr(out["iters"]),
