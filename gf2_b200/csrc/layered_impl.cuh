@@ -95,6 +95,22 @@ __device__ __forceinline__ void st_msg<1>(__half* p, int s, float v) {
   __stcs((unsigned short*)p + s, __half_as_ushort(__float2half_rn(v)));
 }
 
+// Sum-product message of magnitude |v| <= 16.64 (the SFU rows cap it there,
+// far inside binary16's range, so the rounding needs no clamp): stores it
+// through the message type and returns the rounded value, one conversion for
+// both (the result equals st_msg(p, s, IO::rt(v))).
+template <int MSG16>
+__device__ __forceinline__ float put_capped_msg(typename MsgIO<MSG16>::T* p, int s, float v) {
+  if constexpr (MSG16) {
+    const __half h = __float2half_rn(v);
+    __stcs((unsigned short*)p + s, __half_as_ushort(h));
+    return __half2float(h);
+  } else {
+    __stcs(p + s, v);
+    return v;
+  }
+}
+
 // Old messages of one check: slot i at p[i * nchk] of the (streamed) global
 // message array, or at a shared-memory stage that a TMA copy filled.
 template <int MSG16>
@@ -279,7 +295,6 @@ template <int MSG16, int D, bool PART, class OM>
 __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t, int nchk, int s0, float* app,
                                              typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om, bool first,
                                              const LayerSmem& S, int d) {
-  typedef MsgIO<MSG16> IO;
   float x[D], e[D];
 #pragma unroll
   for (int i = 0; i < D; i++) x[i] = (!PART || i < d) ? app[slot_u(__ldg(&sd[i]), t, nchk)] : 3.402823466e38f;
@@ -308,8 +323,7 @@ __device__ __forceinline__ void spa_fast_row(const int2* __restrict__ sd, int t,
     const float den = fmaxf(__fmaf_rn(Dp, ni, -N * di), num * 5.9604645e-08f);
     const float mag = fminf(0.69314718055994531f * lg2_approx(num * rcp_approx(den)), 16.635532f);
     if (!PART || i < d) {
-      const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
-      st_msg<MSG16>(c2v, s0 + i * nchk, out);
+      const float out = put_capped_msg<MSG16>(c2v, s0 + i * nchk, (negp ^ ((neg >> i) & 1u)) ? -mag : mag);
       const float nw = x[i] + out;
       app[slot_u(__ldg(&sd[i]), t, nchk)] = nw;
       flips |= (uint32_t)(((apneg >> i) & 1u) != (uint32_t)(nw < 0.0f)) << i;
@@ -336,7 +350,6 @@ __device__ __forceinline__ void spa_fast_rep_a(const int2* __restrict__ sd, int 
                                                typename MsgIO<MSG16>::T* __restrict__ c2v, const OM& om, bool first,
                                                uint32_t sync, float* dbuf, const LayerSmem& S,
                                                int d) {
-  typedef MsgIO<MSG16> IO;
   const uint32_t rep = sync | (sync << 1);  // slots inside a run
   float x[D], e[D];
 #pragma unroll
@@ -366,8 +379,7 @@ __device__ __forceinline__ void spa_fast_rep_a(const int2* __restrict__ sd, int 
     const float den = fmaxf(__fmaf_rn(Dp, ni, -N * di), num * 5.9604645e-08f);
     const float mag = fminf(0.69314718055994531f * lg2_approx(num * rcp_approx(den)), 16.635532f);
     if (!PART || i < d) {
-      const float out = IO::rt((negp ^ ((neg >> i) & 1u)) ? -mag : mag);
-      st_msg<MSG16>(c2v, s0 + i * nchk, out);
+      const float out = put_capped_msg<MSG16>(c2v, s0 + i * nchk, (negp ^ ((neg >> i) & 1u)) ? -mag : mag);
       const float delta = out - dbuf[i * nchk + t];
       if ((rep >> i) & 1u) {
         dbuf[i * nchk + t] = delta;
