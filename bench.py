@@ -278,7 +278,7 @@ class SingleCode:
                                        want_info=False, want_cw=False)
         msg = g.MSG_F16 if w["msg16"] else g.MSG_F32
         from gf2_b200 import autotune
-        sample = self.llr[:min(2048, self.frames)]
+        sample = self.llr[:min(8192, self.frames)]  # the whole batch up to 8192 frames: its tail counts
         shape, _ = autotune.tune([self.code], w["algo"], w["sched"], msg,
                                  lambda d: d.decode_tensors(sample, w["max_iter"]))
         self.dec = g.LdpcDecoder(self.code, algorithm=w["algo"], schedule=w["sched"], msg_dtype=msg,
