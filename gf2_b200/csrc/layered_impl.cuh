@@ -750,13 +750,14 @@ __device__ __forceinline__ void layered_iterations(const DecodeArgs& a, const De
       } else {
         om = OM{c2v + s0, nchk};
       }
-      // Posteriors in the workspace and no message stage running on the copy
-      // engine: the next row group's slots each read one whole variable group
-      // (Z consecutive posteriors); lane i of the last warp has slot i's group
-      // (lane 31: the compressed states of the row group) prefetched into L2,
-      // so that those gathers wait on L2 rather than DRAM.  (Issued by one
-      // thread in a loop, or next to the sum-product stage copies, it was slower.)
-      if constexpr (!STG || ST) {
+      // Several checks per thread, posteriors in the workspace and no message
+      // stage running on the copy engine: the next row group's slots each read
+      // one whole variable group (Z consecutive posteriors); lane i of the last
+      // warp has slot i's group (lane 31: the compressed states of the row
+      // group) prefetched into L2, so that those gathers wait on L2 rather than
+      // DRAM.  (With one check per thread, issued by one thread in a loop, or
+      // next to the sum-product stage copies, it was slower.)
+      if constexpr ((!STG || ST) && MULTI) {
         if (pf && (tid >> 5) == ((int)blockDim.x >> 5) - 1) {  // lane i of the last warp: slot i
           const int lane = tid & 31;
           const int gn = (g + 1 < ncg) ? g + 1 : 0;
