@@ -64,7 +64,8 @@ def candidates(codes, schedule, msg_dtype=0, algorithm=3):
     to 32), or for one code with FP16 messages and a fused-row algorithm 192 /
     128 threads (each thread two / three checks, so four / six frames in
     flight per SM at the same registers; 192 threads with 5 CTAs per SM is a
-    64-register build); the CTAs per SM vary within what fits.  Flooding: the
+    64-register build), and for a mixed batch with the SFU sum-product 192
+    threads (posteriors in the workspace); the CTAs per SM vary within what fits.  Flooding: the
     library's choice (512 threads, or the check-state kernel of the min-sum
     family) at any / 1 / 2 CTAs per SM, 256 and 384 threads, and 1024 threads
     (codes of check degree <= 8: more threads per frame for small batches).
@@ -73,6 +74,8 @@ def candidates(codes, schedule, msg_dtype=0, algorithm=3):
         c = [(0, b) for b in (0, 1)]
         if len(codes) == 1 and msg_dtype == 1 and algorithm != 1:
             c += [(192, b) for b in (0, 3, 5)] + [(128, b) for b in (0, 4)]
+        elif len(codes) > 1 and msg_dtype == 1 and algorithm == 3:  # mixed batch, SFU sum-product
+            c += [(192, b) for b in (0, 3)]
         return c
     return [(0, 0), (0, 1), (0, 2), (256, 0), (384, 0), (1024, 0)]
 

@@ -386,8 +386,10 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   // thread, more frames in flight per SM) 192 / 128 threads for one code with
   // FP16 messages and a fused-row algorithm, on the TMA-staged kernel.
   const bool multi = layered && threads < d->max_nchk;
-  if (multi && !((threads == 192 || threads == 128) && d->codes.size() == 1 && o.msg_dtype == GF2C_MSG_F16 &&
-                 o.algorithm != GF2C_ALGO_SPA && d->max_nchk <= 384))
+  // a mixed batch: 192 threads for the SFU sum-product (the mixed kernel)
+  const bool multi_mixed = multi && d->codes.size() > 1 && threads == 192 && o.algorithm == GF2C_ALGO_SPA_FAST;
+  if (multi && !((threads == 192 || threads == 128) && (d->codes.size() == 1 || multi_mixed) &&
+                 o.msg_dtype == GF2C_MSG_F16 && o.algorithm != GF2C_ALGO_SPA && d->max_nchk <= 384))
     return set_error(GF2C_ERR_INVALID_ARG,
                      "layered schedule needs threads_per_block >= row group size (or 192 / 128 threads for one "
                      "DVB-T2 code, FP16 messages, min-sum / NMS / SFU sum-product)");
@@ -402,6 +404,9 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
   d->smem_app_floats = 0;
   for (auto* c : d->codes)
     if (smem_of((int)c->h->n) <= (size_t)kSmemBudget) d->smem_app_floats = std::max(d->smem_app_floats, (int)c->h->n);
+  // several checks per thread over a mixed batch: every posterior in the
+  // workspace, so that the CTAs are small enough for four per SM
+  if (multi_mixed) d->smem_app_floats = 0;
   d->smem = smem_of(d->smem_app_floats);
   if (layered && o.algorithm != GF2C_ALGO_SPA) {
     // row groups with repeated variables: deltas of every slot (fused row paths)
@@ -433,7 +438,8 @@ int gf2c_decoder_create_multi(const gf2c_code* const* codes, int32_t ncodes, con
       differ = differ || b != d->dcmax;
       dispatchable = dispatchable && b > 0 && b <= 22;
     }
-    const void* k = (differ && dispatchable) ? layered_kernel_ptr(o.algorithm, o.msg_dtype, 0, threads) : nullptr;
+    const void* k = ((differ || multi_mixed) && dispatchable) ? layered_kernel_ptr(o.algorithm, o.msg_dtype, 0, threads)
+                                                               : nullptr;
     if (k) d->kernel = k;
   }
   // Flooding min-sum / normalised-offset min-sum: the check-state kernel, with

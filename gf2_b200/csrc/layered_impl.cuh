@@ -1087,6 +1087,10 @@ static const void* lay_wide(int dcmax) {
 template <int ALGO, int MSG16>
 static const void* lay_t(int dcmax, int maxt, bool stage, int bps) {
   if (maxt > 384) return stage ? nullptr : lay_wide<ALGO, MSG16>(dcmax);
+  if (dcmax == 0 && maxt == 192 && !stage) {  // mixed batches, two checks per thread
+    if constexpr (ALGO == L_SPA_FAST && MSG16) return (const void*)bp_layered_kernel<ALGO, MSG16, 0, 192, 4, false>;
+    return nullptr;
+  }
   if constexpr (ALGO == L_SPA) {
     return (stage || maxt < 384) ? nullptr : lay_exact<ALGO, MSG16, 1, false>(dcmax);
   } else {

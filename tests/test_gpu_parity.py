@@ -548,3 +548,40 @@ def test_layered_compressed_states_equal_per_edge_messages(gpu, monkeypatch, idx
     for key in ("msg", "iters", "conv", "synd_ok"):
         assert torch.equal(states[key], per_edge[key]), key
     assert torch.equal(states["beliefs"].view(torch.int32), per_edge["beliefs"].view(torch.int32))
+
+
+def test_mixed_batch_two_checks_per_thread(gpu):
+    """A mixed batch at 192 threads (two checks per thread, posteriors in the
+    workspace) gives the one-check-per-thread mixed decoder's results on every
+    frame, short and normal codes, with repeated-variable row groups."""
+    import torch
+    codes = [g.LdpcCode.dvb_t2_short(0), g.LdpcCode.dvb_t2_normal(1), g.LdpcCode.dvb_t2_short(4),
+             g.LdpcCode.dvb_t2_normal(5)]
+    kw = dict(algorithm=g.ALGO_SPA_FAST, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16)
+    rng = np.random.default_rng(21)
+    F = 1200
+    cid = rng.integers(0, 4, F).astype(np.int32)
+    mit = rng.integers(5, 40, F).astype(np.int32)
+    ebn0 = [1.2, 1.1, 2.6, 3.3]
+    parts, lo, base = [], np.zeros(F, np.int64), 0
+    for c in range(4):
+        idx = np.nonzero(cid == c)[0]
+        s2 = np.array([g.sigma2_from_ebn0(ebn0[c] + 0.1 * (i % 5), codes[c].rate()) for i in idx])
+        _, _, l = g.awgn_frames(codes[c], 23, c << 20, len(idx), s2, device=gpu, want_info=False, want_cw=False)
+        parts.append(l.reshape(-1))
+        lo[idx] = base + np.arange(len(idx)) * codes[c].n()
+        base += len(idx) * codes[c].n()
+    llr = torch.cat(parts)
+    W = max(g.words(c.k()) for c in codes)
+    dt = lambda x: torch.from_numpy(x).to(gpu)
+    res = []
+    for threads in (0, 192):
+        dec = g.LdpcDecoder(codes[0], codes=codes, threads_per_block=threads, **kw)
+        o = dict(msg=torch.zeros(F * W, dtype=torch.int64, device=gpu), it=torch.zeros(F, dtype=torch.int32, device=gpu),
+                 cv=torch.zeros(F, dtype=torch.uint8, device=gpu), so=torch.zeros(F, dtype=torch.uint8, device=gpu))
+        dec.decode_mixed_tensors(llr, dt(lo), dt(cid), dt(mit), o["msg"], dt(np.arange(F, dtype=np.int64) * W), o["it"],
+                                 o["cv"], o["so"], use_graph=False)
+        torch.cuda.synchronize()
+        res.append(o)
+    for k in ("msg", "it", "cv", "so"):
+        assert torch.equal(res[0][k], res[1][k]), k
