@@ -280,7 +280,7 @@ class SingleCode:
         from gf2_b200 import autotune
         sample = self.llr[:min(8192, self.frames)]  # the whole batch up to 8192 frames: its tail counts
         shape, _ = autotune.tune([self.code], w["algo"], w["sched"], msg,
-                                 lambda d: d.decode_tensors(sample, w["max_iter"]))
+                                 lambda d: d.decode_tensors(sample, w["max_iter"]), frames=sample.shape[0])
         self.dec = g.LdpcDecoder(self.code, algorithm=w["algo"], schedule=w["sched"], msg_dtype=msg,
                                  threads_per_block=shape[0], blocks_per_sm=shape[1])
         self.out = None
@@ -378,7 +378,8 @@ class Mixed:
         def run(dec):
             dec.decode_mixed_tensors(self.llr, self.llr_off, self.cid, self.mit, self.msg, self.msg_off,
                                      self.iters, self.conv, self.so, use_graph=False)
-        (threads, bps), self.tune_table = autotune.tune(self.codes, self.algo, self.sched, self.msg16, run)
+        (threads, bps), self.tune_table = autotune.tune(self.codes, self.algo, self.sched, self.msg16, run,
+                                                        frames=self.frames)
         self.shape = (threads, bps)
         self.dec = g.LdpcDecoder(self.codes[0], codes=self.codes, algorithm=self.algo, schedule=self.sched,
                                  msg_dtype=self.msg16, threads_per_block=threads, blocks_per_sm=bps)
@@ -473,9 +474,10 @@ class LearnedScale:
         kw_nms = dict(algorithm=g.ALGO_NMS, schedule=g.SCHED_LAYERED, nms_alpha=a, nms_beta=b, msg_dtype=g.MSG_F16)
         kw_spa = dict(algorithm=g.ALGO_SPA_FAST, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16)
         sh_nms, _ = autotune.tune([self.code], g.ALGO_NMS, g.SCHED_LAYERED, g.MSG_F16,
-                                  lambda d: d.decode_tensors(sample, self.T), nms_alpha=a, nms_beta=b)
+                                  lambda d: d.decode_tensors(sample, self.T), nms_alpha=a, nms_beta=b,
+                                  frames=sample.shape[0])
         sh_spa, _ = autotune.tune([self.code], g.ALGO_SPA_FAST, g.SCHED_LAYERED, g.MSG_F16,
-                                  lambda d: d.decode_tensors(sample, 50))
+                                  lambda d: d.decode_tensors(sample, 50), frames=sample.shape[0])
         self.shapes = {"learned": sh_nms, "plain": sh_spa}
         self.nms = g.LdpcDecoder(self.code, threads_per_block=sh_nms[0], blocks_per_sm=sh_nms[1], **kw_nms)
         self.spa = g.LdpcDecoder(self.code, threads_per_block=sh_spa[0], blocks_per_sm=sh_spa[1], **kw_spa)

@@ -6,9 +6,9 @@ thread steps over in each row group (the tile) and the number of frames in
 flight per SM.
 The autotuner times every feasible shape on a sample batch with CUDA events
 and keeps the fastest; results are cached in a JSON file keyed by device name,
-the build of the library (a hash of libgf2cuda.so), codes, algorithm, schedule
-and message type (GF2C_AUTOTUNE_CACHE overrides the default
-~/.cache/gf2_b200/autotune.json).
+the build of the library (a hash of libgf2cuda.so), codes, algorithm, schedule,
+message type and the sample's frame count (GF2C_AUTOTUNE_CACHE overrides the
+default ~/.cache/gf2_b200/autotune.json).
 """
 import json
 import os
@@ -53,9 +53,10 @@ def library_hash():
     return _LIB_HASH
 
 
-def _key(codes, algorithm, schedule, msg_dtype, device_name):
+def _key(codes, algorithm, schedule, msg_dtype, device_name, frames=None):
     cs = ",".join(f"{c.n()}x{c.m()}x{c.nnz()}" for c in codes)
-    return f"{device_name}|lib {library_hash()}|{cs}|a{algorithm}|s{schedule}|m{msg_dtype}"
+    fs = f"|f{frames}" if frames else ""  # a shape timed on a few frames is not reused for many
+    return f"{device_name}|lib {library_hash()}|{cs}|a{algorithm}|s{schedule}|m{msg_dtype}{fs}"
 
 
 def candidates(codes, schedule, msg_dtype=0, algorithm=3):
@@ -80,12 +81,14 @@ def candidates(codes, schedule, msg_dtype=0, algorithm=3):
     return [(0, 0), (0, 1), (0, 2), (256, 0), (384, 0), (1024, 0)]
 
 
-def tune(codes, algorithm, schedule, msg_dtype, run, reps=3, nms_alpha=None, nms_beta=None, force=False):
+def tune(codes, algorithm, schedule, msg_dtype, run, reps=3, nms_alpha=None, nms_beta=None, force=False,
+         frames=None):
     """Return ((threads, blocks_per_sm), table).  `run(decoder)` decodes the
-    sample batch once on the current stream."""
+    sample batch once on the current stream; `frames` (its size) is part of the
+    cache key, since the best shape depends on how many frames are in flight."""
     import torch
     dev_name = torch.cuda.get_device_name()
-    key = _key(codes, algorithm, schedule, msg_dtype, dev_name)
+    key = _key(codes, algorithm, schedule, msg_dtype, dev_name, frames)
     cache = _load()
     if key in cache and not force:
         e = cache[key]
