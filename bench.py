@@ -99,6 +99,10 @@ def data_of(w, gpu_arm):
             else "synthetic (seeded Philox AWGN frames)")
 
 
+# (threads, CTAs per SM) of the workload's primary decoder from --shape, else None (autotuned)
+FORCED_SHAPE = None
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -107,6 +111,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="c5", choices=WORKLOADS)
     p.add_argument("--frames", type=int, default=0, help="override frames per rank (profiling)")
+    p.add_argument("--shape", default=None,
+                   help="THREADS,CTAS_PER_SM: launch shape of the workload's (primary) decoder instead of the "
+                        "autotuner's (profiling a small case at the full run's shape)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args()
@@ -279,8 +286,9 @@ class SingleCode:
         msg = g.MSG_F16 if w["msg16"] else g.MSG_F32
         from gf2_b200 import autotune
         sample = self.llr[:min(8192, self.frames)]  # the whole batch up to 8192 frames: its tail counts
-        shape, _ = autotune.tune([self.code], w["algo"], w["sched"], msg,
-                                 lambda d: d.decode_tensors(sample, w["max_iter"]), frames=sample.shape[0])
+        shape = FORCED_SHAPE or autotune.tune([self.code], w["algo"], w["sched"], msg,
+                                              lambda d: d.decode_tensors(sample, w["max_iter"]),
+                                              frames=sample.shape[0])[0]
         self.dec = g.LdpcDecoder(self.code, algorithm=w["algo"], schedule=w["sched"], msg_dtype=msg,
                                  threads_per_block=shape[0], blocks_per_sm=shape[1])
         self.out = None
@@ -378,8 +386,11 @@ class Mixed:
         def run(dec):
             dec.decode_mixed_tensors(self.llr, self.llr_off, self.cid, self.mit, self.msg, self.msg_off,
                                      self.iters, self.conv, self.so, use_graph=False)
-        (threads, bps), self.tune_table = autotune.tune(self.codes, self.algo, self.sched, self.msg16, run,
-                                                        frames=self.frames)
+        if FORCED_SHAPE:
+            (threads, bps), self.tune_table = FORCED_SHAPE, []
+        else:
+            (threads, bps), self.tune_table = autotune.tune(self.codes, self.algo, self.sched, self.msg16, run,
+                                                            frames=self.frames)
         self.shape = (threads, bps)
         self.dec = g.LdpcDecoder(self.codes[0], codes=self.codes, algorithm=self.algo, schedule=self.sched,
                                  msg_dtype=self.msg16, threads_per_block=threads, blocks_per_sm=bps)
@@ -473,9 +484,9 @@ class LearnedScale:
         sample = self.llr[:min(8192, self.frames)]
         kw_nms = dict(algorithm=g.ALGO_NMS, schedule=g.SCHED_LAYERED, nms_alpha=a, nms_beta=b, msg_dtype=g.MSG_F16)
         kw_spa = dict(algorithm=g.ALGO_SPA_FAST, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16)
-        sh_nms, _ = autotune.tune([self.code], g.ALGO_NMS, g.SCHED_LAYERED, g.MSG_F16,
-                                  lambda d: d.decode_tensors(sample, self.T), nms_alpha=a, nms_beta=b,
-                                  frames=sample.shape[0])
+        sh_nms = FORCED_SHAPE or autotune.tune([self.code], g.ALGO_NMS, g.SCHED_LAYERED, g.MSG_F16,
+                                               lambda d: d.decode_tensors(sample, self.T), nms_alpha=a, nms_beta=b,
+                                               frames=sample.shape[0])[0]
         sh_spa, _ = autotune.tune([self.code], g.ALGO_SPA_FAST, g.SCHED_LAYERED, g.MSG_F16,
                                   lambda d: d.decode_tensors(sample, 50), frames=sample.shape[0])
         self.shapes = {"learned": sh_nms, "plain": sh_spa}
@@ -833,6 +844,9 @@ def make_workload(name, dev, rank, frames):
 
 def main():
     args = parse()
+    global FORCED_SHAPE
+    if args.shape:
+        FORCED_SHAPE = tuple(int(x) for x in args.shape.split(","))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
