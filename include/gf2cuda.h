@@ -29,7 +29,9 @@
  *     gf2c_decode_batch splits host-memory batches of 64 MB of LLRs and more
  *     into chunks that alternate between `stream` and a second stream of the
  *     decoder (its own workspace), so that copies overlap decoding; pinned
- *     host memory lets the copies run asynchronously.
+ *     host memory lets the copies run asynchronously.  A host-memory call
+ *     stages the whole batch in device memory (GF2C_ERR_NOMEM when it does
+ *     not fit: split such a batch into several calls).
  *     Host-memory calls return after the results are in host memory;
  *     device-memory calls are asynchronous on `stream`.
  *   - Code handles are immutable after creation and may be shared by threads.
