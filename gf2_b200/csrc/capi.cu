@@ -36,6 +36,11 @@ struct DevBuf {
     bytes = 0;
     size_t sz = std::max(need, (size_t)256);
     cudaError_t e = cudaMalloc(&p, sz);
+    if (e == cudaErrorMemoryAllocation) {  // not sticky: the context stays usable
+      cudaGetLastError();
+      p = nullptr;
+      return set_error(GF2C_ERR_NOMEM, "out of device memory (" + std::to_string(sz) + " bytes)");
+    }
     if (e != cudaSuccess) return cuda_error(e, "cudaMalloc");
     bytes = sz;
     return GF2C_OK;
