@@ -439,9 +439,10 @@ __device__ __forceinline__ void ms_row(const int2* __restrict__ sd, int t, int n
     if (PART && i >= d) continue;
     const float w = __fsub_rn(ap[i], o[i]);
     const float ax = fabsf(w);
-    // the two smallest magnitudes and the first argmin, branch-free
+    // the two smallest magnitudes and the first argmin, branch-free (a NaN
+    // magnitude changes none of them, as with the comparisons of the rule)
     i1 = (ax < m1) ? i : i1;
-    m2 = fminf(m2, fmaxf(m1, ax));
+    m2 = fmaxf(m1, fminf(m2, ax));
     m1 = fminf(m1, ax);
     neg |= (uint32_t)(w < 0.0f) << i;
     apneg |= (uint32_t)(ap[i] < 0.0f) << i;

@@ -585,3 +585,37 @@ def test_mixed_batch_two_checks_per_thread(gpu):
         res.append(o)
     for k in ("msg", "it", "cv", "so"):
         assert torch.equal(res[0][k], res[1][k]), k
+
+
+@pytest.mark.parametrize("msg16", [True, False])
+def test_layered_nms_special_llrs_equal_oracle(gpu, oracle, msg16):
+    """Layered normalised / offset min-sum with +-inf, NaN and +-0 channel
+    values among ordinary ones: iterations, flags and decisions equal the
+    oracle's, posteriors bitwise equal where the oracle's is a number and NaN
+    where it is NaN (a NaN magnitude is never a check's minimum on either
+    side)."""
+    code = g.LdpcCode.dvb_t2_short(g.CodeRate.Rate1_2)
+    ocode = oracle.Code.dvbt2(1, 0)
+    _, _, llr = ocode.channel(31, 0, 12, 2.0)
+    llr = llr.copy()
+    rng = np.random.default_rng(8)
+    for f in range(12):
+        idx = rng.choice(code.n(), 40, replace=False)
+        llr[f, idx[:10]] = np.inf
+        llr[f, idx[10:20]] = -np.inf
+        llr[f, idx[20:25]] = np.nan if f % 3 == 0 else 0.0
+        llr[f, idx[25:30]] = -0.0
+    T, L = 6, code.layers()
+    a = (0.7 + 0.3 * rng.random((T, L))).astype(np.float32)
+    b = (0.3 * rng.random((T, L))).astype(np.float32)
+    kw = dict(algorithm=g.ALGO_NMS, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16 if msg16 else g.MSG_F32,
+              nms_alpha=a, nms_beta=b)
+    r = g.LdpcDecoder(code, **kw).decode_arrays(llr, 15, beliefs=True)
+    o = ocode.decode(llr, 15, algo=3, sched=1, msg16=msg16, alpha=a, beta=b)
+    assert (r["iters"] == o["iters"]).all() and (r["conv"] == o["conv"]).all()
+    assert (r["synd_ok"] == o["synd_ok"]).all()
+    assert (unpack_msg(r, code.k()) == o["msg"]).all()
+    gb, ob = r["beliefs"], o["beliefs"]
+    nan = np.isnan(ob)
+    assert (np.isnan(gb) == nan).all()
+    assert (gb[~nan].view(np.uint32) == ob[~nan].view(np.uint32)).all()
