@@ -83,9 +83,12 @@ struct gf2c_decoder {
   cudaStream_t gstream = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   // pipelined host-memory batches: a second decode stream with its own
-  // workspace and queue, and a stream that issues the input copies
-  cudaStream_t pstream = nullptr, cstream = nullptr;
+  // workspace and queue, and a stream that issues the input copies; the
+  // fallback call's high-priority stream for the fallback passes and the
+  // output copies (each chunk's after its primary pass, event pev_prim)
+  cudaStream_t pstream = nullptr, cstream = nullptr, fstream = nullptr;
   cudaEvent_t pev_fork = nullptr, pev_join = nullptr, pev_copy[2] = {nullptr, nullptr};
+  cudaEvent_t pev_prim = nullptr, pev_fjoin = nullptr;
   DevBuf work2, queue2;
   // mixed batches: rank of each code in the frame order (longest codes first),
   // frame order buffer; host copy of the ranks and the per-chunk frame counts
@@ -102,14 +105,14 @@ struct gf2c_decoder {
       cudaStreamSynchronize(gstream);
       cudaStreamDestroy(gstream);
     }
-    for (cudaStream_t ps : {pstream, cstream})
+    for (cudaStream_t ps : {pstream, cstream, fstream})
       if (ps) {
         cudaStreamSynchronize(ps);
         cudaStreamDestroy(ps);
       }
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
-    for (cudaEvent_t e : {pev_fork, pev_join, pev_copy[0], pev_copy[1]})
+    for (cudaEvent_t e : {pev_fork, pev_join, pev_copy[0], pev_copy[1], pev_prim, pev_fjoin})
       if (e) cudaEventDestroy(e);
   }
 };
@@ -645,17 +648,21 @@ static int check_status(gf2c_decoder* d, cudaStream_t st) {
   return GF2C_OK;
 }
 
-// Chunk sizes of the pipelined host-memory paths: one wave of frames first
-// (the copy that nothing overlaps is short), then doubling up to an eighth of
-// the batch, so that each copy is done before the SMs run out of work both when
-// decoding is much slower than the copy and when it runs at about the copy's
-// speed (the last chunk's decode, after the last copy, is then short); a
-// remainder below one wave joins the last chunk.
+// Chunk sizes of the pipelined host-memory paths.  Mixed batches: one wave of
+// frames first (the copy that nothing overlaps is short), then doubling up to
+// an eighth of the batch.  Single-code batches: chunks of one size, the larger
+// of one wave and a 64th of the batch, so that the copy of the first chunk and
+// the decode of the last one (what the copies cannot overlap) are short, and
+// each chunk's copy takes about as long as the previous chunk's decode when
+// the two run at about the same speed (the copy stream then stays busy from
+// the first copy to the last).  A remainder below one wave joins the last
+// chunk.
 static int64_t chunk_frames(int64_t want, int64_t left, int64_t wave) {
   const int64_t nf = std::min(want, left);
   return (left - nf < wave) ? left : nf;
 }
 static int64_t chunk_cap(int64_t frames, int64_t wave) { return std::max(wave, (frames + 7) / 8); }
+static int64_t even_chunk(int64_t frames, int64_t wave) { return std::max(wave, (frames + 63) / 64); }
 
 // The second decode stream, its workspace and queue, and the copy stream of
 // the pipelined host-memory path (made on first use; false where they cannot
@@ -716,16 +723,18 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
   // buffer holds the whole batch, so no copy waits for a decode).  A chunk's
   // decode waits for its own copy only and starts on the SMs that the previous
   // chunk's last frames leave free (each stream has its own workspace and
-  // frame queue).
+  // frame queue).  Only the last chunk is decoded hardest frames first: the
+  // ordering kernels of the others would wait for those SMs, which the next
+  // chunk's decode fills anyway.
   const int64_t chunk = std::max<int64_t>(dec->grid, (frames + 7) / 8);
   if (frames >= 2 * chunk && bl >= ((size_t)64 << 20) && pipeline_ready(dec)) {
     GF2C_CUDA(cudaEventRecord(dec->pev_fork, st));
     GF2C_CUDA(cudaStreamWaitEvent(dec->pstream, dec->pev_fork, 0));
     GF2C_CUDA(cudaStreamWaitEvent(dec->cstream, dec->pev_fork, 0));
     int chunks = 0, launches = 0;
-    const int64_t cap = chunk_cap(frames, dec->grid);
-    for (int64_t f0 = 0, nf = 0, want = dec->grid; f0 < frames; f0 += nf, chunks++, want = std::min(2 * want, cap)) {
-      nf = chunk_frames(want, frames - f0, dec->grid);
+    const int64_t csz = even_chunk(frames, dec->grid);
+    for (int64_t f0 = 0, nf = 0; f0 < frames; f0 += nf, chunks++) {
+      nf = chunk_frames(csz, frames - f0, dec->grid);
       const int slot = chunks & 1;
       cudaStream_t s = slot ? dec->pstream : st;
       const size_t ln = (size_t)nf * h.n * 4, lo = (size_t)f0 * h.n * 4;
@@ -744,7 +753,7 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
       b.synd_ok = (uint8_t*)dec->s_so.p + f0;
       b.beliefs = beliefs ? (float*)((char*)dec->s_bel.p + lo) : nullptr;
       int extra = 0;
-      if ((rc = key_order(dec, b, nf, s, slot, extra))) return rc;
+      if (f0 + nf == frames && (rc = key_order(dec, b, nf, s, slot, extra))) return rc;
       if ((rc = launch_decoder(dec, b, nf, s, slot))) return rc;
       launches += 1 + extra;
       if (msg_bits)
@@ -782,28 +791,65 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
   return check_status(dec, st);
 }
 
-// One primary pass, failed-frame list and fallback pass over `frames` frames
-// whose arrays `a` points at, on stream `st` (slot: workspace and queue of the
-// pipelined host path); the list goes to `list`, its length to *cnt.
+// The primary pass over `frames` frames whose arrays `a` points at, on stream
+// `st` (slot: workspace and queue of the pipelined host path); `ordered`:
+// hardest frames first (key_order).
+static int primary_pass(gf2c_decoder* primary, DecodeArgs a, int64_t frames, int32_t max_iter_primary,
+                        cudaStream_t st, int slot, int& launches, bool ordered = true) {
+  int rc, extra = 0;
+  a.max_iter = max_iter_primary;
+  if (ordered && (rc = key_order(primary, a, frames, st, slot, extra))) return rc;
+  if ((rc = launch_decoder(primary, a, frames, st, slot))) return rc;
+  launches += 1 + extra;
+  return GF2C_OK;
+}
+// The frames the primary pass left failing, listed on the device (the list
+// goes to `list`, its length to *cnt), and the fallback decoder on them (the
+// count read on the device), on stream `st`.
+static int fallback_pass(gf2c_decoder* fallback, DecodeArgs a, int64_t frames, int32_t max_iter_primary,
+                         int32_t max_iter_fallback, int64_t* list, long long* cnt, cudaStream_t st, int slot,
+                         int& launches) {
+  GF2C_CUDA(launch_failed_list(a.synd_ok, frames, list, cnt, st));
+  a.max_iter = max_iter_fallback;
+  a.order = list;
+  a.frames_dev = cnt;
+  a.iters_add = max_iter_primary;
+  int rc = launch_decoder(fallback, a, frames, st, slot);
+  if (rc) return rc;
+  launches += 2;
+  return GF2C_OK;
+}
+// Both passes on one stream.
 static int fallback_passes(gf2c_decoder* primary, gf2c_decoder* fallback, DecodeArgs a, int64_t frames,
                            int32_t max_iter_primary, int32_t max_iter_fallback, int64_t* list, long long* cnt,
                            cudaStream_t st, int slot, int& launches) {
-  int rc, extra = 0;
-  // 1. the primary decoder on every frame
-  a.max_iter = max_iter_primary;
-  if ((rc = key_order(primary, a, frames, st, slot, extra))) return rc;
-  if ((rc = launch_decoder(primary, a, frames, st, slot))) return rc;
-  // 2. the frames it left failing, listed on the device
-  GF2C_CUDA(launch_failed_list(a.synd_ok, frames, list, cnt, st));
-  // 3. the fallback decoder on the listed frames (count read on the device)
-  DecodeArgs b = a;
-  b.max_iter = max_iter_fallback;
-  b.order = list;
-  b.frames_dev = cnt;
-  b.iters_add = max_iter_primary;
-  if ((rc = launch_decoder(fallback, b, frames, st, slot))) return rc;
-  launches = 3 + extra;
-  return GF2C_OK;
+  int rc;
+  launches = 0;
+  if ((rc = primary_pass(primary, a, frames, max_iter_primary, st, slot, launches))) return rc;
+  return fallback_pass(fallback, a, frames, max_iter_primary, max_iter_fallback, list, cnt, st, slot, launches);
+}
+
+// The fallback call's stream for the fallback passes of a pipelined host batch
+// (the highest priority, so that the few frames of a fallback pass get SMs as
+// soon as the primary passes free them) and its events; false where they
+// cannot be had.
+static bool fallback_stream_ready(gf2c_decoder* d) {
+  if (!d->fstream) {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&d->fstream, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+      d->fstream = nullptr;
+      cudaGetLastError();
+      return false;
+    }
+  }
+  for (cudaEvent_t* e : {&d->pev_prim, &d->pev_fjoin})
+    if (!*e && cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) {
+      *e = nullptr;
+      cudaGetLastError();
+      return false;
+    }
+  return true;
 }
 
 int gf2c_decode_batch_fallback(gf2c_decoder* primary, gf2c_decoder* fallback, const float* llr, int64_t frames,
@@ -850,7 +896,16 @@ int gf2c_decode_batch_fallback(gf2c_decoder* primary, gf2c_decoder* fallback, co
   // Host memory: the batch is staged in the primary decoder's buffers.  Large
   // batches go in chunks alternating between the caller's stream and a second
   // stream, as in gf2c_decode_batch, with the input copies issued back to back
-  // on a copy stream.  Every chunk has its own list and count.
+  // on a copy stream, and only the last chunk decoded hardest frames first.
+  // The fallback passes and output copies run on a third stream, one per group
+  // of chunks (about eight groups), each after its chunks' primary passes
+  // only, so that the primary passes follow one another without waiting for
+  // the fallback passes (a few frames of up to max_iter_fallback iterations
+  // each: a pass lasts about as long whatever its frame count, so fewer passes
+  // finish sooner).  The fallback passes share the fallback decoder's first
+  // workspace, one after another on that stream; every group has its own list
+  // and count.  When the two decoders are one, each chunk's passes stay on its
+  // own stream and workspace.
   const HostCode& h = *primary->codes[0]->h;
   const int wk = (int)((h.k + 63) / 64);
   const size_t bl = (size_t)frames * h.n * 4, bm = (size_t)frames * wk * 8;
@@ -861,21 +916,22 @@ int gf2c_decode_batch_fallback(gf2c_decoder* primary, gf2c_decoder* fallback, co
     return rc;
   const int64_t wave = std::max(primary->grid, fallback->grid);
   const bool pipe = frames >= 3 * wave && bl >= ((size_t)64 << 20) && pipeline_ready(primary) &&
-                    pipeline_ready(fallback);
+                    (fallback == primary || fallback_stream_ready(primary));
+  const bool fsplit = pipe && fallback != primary;
   if (pipe) {
     GF2C_CUDA(cudaEventRecord(primary->pev_fork, st));
     GF2C_CUDA(cudaStreamWaitEvent(primary->pstream, primary->pev_fork, 0));
     GF2C_CUDA(cudaStreamWaitEvent(primary->cstream, primary->pev_fork, 0));
   }
-  int chunks = 0;
-  const int64_t cap = chunk_cap(frames, wave);
-  for (int64_t f0 = 0, nf = 0, want = pipe ? wave : frames; f0 < frames;
-       f0 += nf, chunks++, want = std::min(2 * want, cap)) {
-    nf = (chunks == 63) ? frames - f0 : chunk_frames(want, frames - f0, wave);
+  int chunks = 0, groups = 0;
+  const int64_t csz = pipe ? even_chunk(frames, wave) : frames;
+  const int gsz = fsplit ? (int)std::max<int64_t>(1, (frames / csz + 7) / 8) : 1;  // chunks per group
+  for (int64_t f0 = 0, nf = 0, g0 = 0; f0 < frames; f0 += nf, chunks++) {
+    nf = (chunks == 63) ? frames - f0 : chunk_frames(csz, frames - f0, wave);
     const int slot = pipe ? (chunks & 1) : 0;
     cudaStream_t s = slot ? primary->pstream : st;
     const size_t ln = (size_t)nf * h.n * 4, lo = (size_t)f0 * h.n * 4;
-    const size_t mn = (size_t)nf * wk * 8, mo = (size_t)f0 * wk * 8;
+    const size_t mo = (size_t)f0 * wk * 8;
     // input copies back to back on the copy stream, each chunk's passes
     // waiting for its own copy only
     if (pipe) {
@@ -892,32 +948,51 @@ int gf2c_decode_batch_fallback(gf2c_decoder* primary, gf2c_decoder* fallback, co
     a.iters = (int32_t*)primary->s_it.p + f0;
     a.conv = (uint8_t*)primary->s_cv.p + f0;
     a.synd_ok = (uint8_t*)primary->s_so.p + f0;
-    int nl = 0;
-    if ((rc = fallback_passes(primary, fallback, a, nf, max_iter_primary, max_iter_fallback,
-                              (int64_t*)primary->fb_list.p + f0, (long long*)primary->fb_count.p + chunks, s, slot,
-                              nl)))
+    if ((rc = primary_pass(primary, a, nf, max_iter_primary, s, slot, launches, f0 + nf == frames))) return rc;
+    if (fsplit) {
+      GF2C_CUDA(cudaEventRecord(primary->pev_prim, s));
+      GF2C_CUDA(cudaStreamWaitEvent(primary->fstream, primary->pev_prim, 0));
+      s = primary->fstream;
+    }
+    if (f0 + nf < frames && (chunks + 1) % gsz != 0) continue;
+    // the group [g0, f0 + nf): fallback pass, then its outputs
+    const int64_t gn = f0 + nf - g0;
+    const size_t gmn = (size_t)gn * wk * 8, gmo = (size_t)g0 * wk * 8;
+    DecodeArgs ga = a;
+    ga.llr = (const float*)((char*)primary->s_llr.p + (size_t)g0 * h.n * 4);
+    ga.msg = msg_bits ? (uint64_t*)((char*)primary->s_msg.p + gmo) : nullptr;
+    ga.iters = (int32_t*)primary->s_it.p + g0;
+    ga.conv = (uint8_t*)primary->s_cv.p + g0;
+    ga.synd_ok = (uint8_t*)primary->s_so.p + g0;
+    if ((rc = fallback_pass(fallback, ga, gn, max_iter_primary, max_iter_fallback, (int64_t*)primary->fb_list.p + g0,
+                            (long long*)primary->fb_count.p + groups, s, fsplit ? 0 : slot, launches)))
       return rc;
-    launches += nl;
     if (msg_bits)
-      GF2C_CUDA(cudaMemcpyAsync((char*)msg_bits + mo, (char*)primary->s_msg.p + mo, mn, cudaMemcpyDeviceToHost, s));
+      GF2C_CUDA(cudaMemcpyAsync((char*)msg_bits + gmo, (char*)primary->s_msg.p + gmo, gmn, cudaMemcpyDeviceToHost, s));
     if (iterations)
-      GF2C_CUDA(cudaMemcpyAsync(iterations + f0, (int32_t*)primary->s_it.p + f0, nf * 4, cudaMemcpyDeviceToHost, s));
+      GF2C_CUDA(cudaMemcpyAsync(iterations + g0, (int32_t*)primary->s_it.p + g0, gn * 4, cudaMemcpyDeviceToHost, s));
     if (converged)
-      GF2C_CUDA(cudaMemcpyAsync(converged + f0, (uint8_t*)primary->s_cv.p + f0, nf, cudaMemcpyDeviceToHost, s));
+      GF2C_CUDA(cudaMemcpyAsync(converged + g0, (uint8_t*)primary->s_cv.p + g0, gn, cudaMemcpyDeviceToHost, s));
     if (syndrome_ok)
-      GF2C_CUDA(cudaMemcpyAsync(syndrome_ok + f0, (uint8_t*)primary->s_so.p + f0, nf, cudaMemcpyDeviceToHost, s));
+      GF2C_CUDA(cudaMemcpyAsync(syndrome_ok + g0, (uint8_t*)primary->s_so.p + g0, gn, cudaMemcpyDeviceToHost, s));
+    groups++;
+    g0 = f0 + nf;
   }
   if (pipe) {
     GF2C_CUDA(cudaEventRecord(primary->pev_join, primary->pstream));
     GF2C_CUDA(cudaStreamWaitEvent(st, primary->pev_join, 0));
   }
+  if (fsplit) {
+    GF2C_CUDA(cudaEventRecord(primary->pev_fjoin, primary->fstream));
+    GF2C_CUDA(cudaStreamWaitEvent(st, primary->pev_fjoin, 0));
+  }
   long long counts[64] = {0};
-  GF2C_CUDA(cudaMemcpyAsync(counts, primary->fb_count.p, sizeof(long long) * chunks, cudaMemcpyDeviceToHost, st));
+  GF2C_CUDA(cudaMemcpyAsync(counts, primary->fb_count.p, sizeof(long long) * groups, cudaMemcpyDeviceToHost, st));
   primary->last_launches = launches;
   if ((rc = check_status(primary, st)) || (rc = check_status(fallback, st))) return rc;
   if (fallback_count) {
     long long total = 0;
-    for (int c = 0; c < chunks; c++) total += counts[c];
+    for (int c = 0; c < groups; c++) total += counts[c];
     *fallback_count = total;
   }
   return GF2C_OK;

@@ -193,8 +193,9 @@ int gf2c_decode_batch(gf2c_decoder* dec, const float* llr, int64_t frames, int32
  *     too); asynchronous on `stream`; 3 or 5 kernel launches.
  *   mem == GF2C_MEM_HOST: every pointer is host memory (pinned memory copies
  *     fastest); the batch is copied in, decoded and copied out, large batches
- *     in chunks on two streams so that copies overlap decoding; returns when
- *     the results are in host memory. */
+ *     in chunks on two streams so that copies overlap decoding (the fallback
+ *     passes and output copies on a third stream of the primary decoder, one
+ *     per group of chunks); returns when the results are in host memory. */
 int gf2c_decode_batch_fallback(gf2c_decoder* primary, gf2c_decoder* fallback, const float* llr, int64_t frames,
                                int32_t max_iter_primary, int32_t max_iter_fallback, uint64_t* msg_bits,
                                int32_t* iterations, uint8_t* converged, uint8_t* syndrome_ok,

@@ -56,10 +56,12 @@ def test_fallback_argument_checks(gpu):
         da.decode_with_fallback(flood, llr, 5, 10)  # fallback not layered
 
 
-@pytest.mark.parametrize("frames", [40, 1000])
+@pytest.mark.parametrize("frames", [40, 1000, 2800])
 def test_fallback_host_memory_equals_device(gpu, frames):
-    """The host-memory call (pinned buffers; 1000 normal frames go in two
-    chunks on two streams) gives the device call's results and count."""
+    """The host-memory call gives the device call's results and count: 40
+    frames in one piece; 1000 normal frames in three chunks on two streams,
+    one fallback pass per chunk; 2800 in nine chunks whose fallback passes
+    run per group of two chunks on the fallback stream."""
     code = g.LdpcCode.dvb_t2_normal(g.CodeRate.Rate2_3)
     L, T = code.layers(), 10
     prim = g.LdpcDecoder(code, algorithm=g.ALGO_NMS, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16,
