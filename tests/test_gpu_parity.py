@@ -201,9 +201,10 @@ def test_device_tensor_path_matches_host(gpu, oracle):
 
 @pytest.mark.parametrize("kw", [dict(), dict(algorithm=g.ALGO_SPA_FAST, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16)])
 def test_pipelined_host_path_matches_device(gpu, kw):
-    """Host-memory batches of 64 MB and more run in chunks on two streams (copies
-    overlapping the decode), batches of more frames than CTAs hardest frames
-    first: every output equals the one-launch device path and small batches."""
+    """Host-memory batches of 64 MB and more run in equal chunks on two streams
+    (copies overlapping the decode, the last chunk hardest frames first);
+    device batches of more frames than CTAs run hardest frames first: every
+    output equals the one-launch device path and small batches."""
     import torch
     code = g.LdpcCode.dvb_t2_short(g.CodeRate.Rate3_5)
     F = 2048  # 133 MB of LLRs
