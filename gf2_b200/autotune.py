@@ -11,6 +11,7 @@ message type and the sample's frame count (GF2C_AUTOTUNE_CACHE overrides the
 default ~/.cache/gf2_b200/autotune.json).
 """
 import json
+import math
 import os
 
 from .ldpc import LdpcDecoder
@@ -104,13 +105,22 @@ def tune(codes, algorithm, schedule, msg_dtype, run, reps=3, nms_alpha=None, nms
             continue
         run(dec)
         torch.cuda.synchronize()
+        # the median of at least `reps` timed runs and of about 100 ms of
+        # decoding (a small batch takes a few milliseconds, too short for 3
+        # runs to separate shapes that differ by a few percent)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
-        for _ in range(reps):
-            run(dec)
+        run(dec)
         ev1.record()
         torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1) / reps
+        n = max(reps, min(64, int(math.ceil(100.0 / max(ev0.elapsed_time(ev1), 1e-3)))))
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(n + 1)]
+        ev[0].record()
+        for i in range(n):
+            run(dec)
+            ev[i + 1].record()
+        torch.cuda.synchronize()
+        ms = sorted(ev[i].elapsed_time(ev[i + 1]) for i in range(n))[n // 2]
         table.append([threads, bps, ms])
         if best is None or ms < best[2]:
             best = (threads, bps, ms)
