@@ -82,3 +82,22 @@ def test_fallback_host_memory_equals_device(gpu, frames):
     hn = prim.decode_with_fallback(fb, llr.cpu().numpy(), T, 50)
     assert isinstance(hn["msg"], np.ndarray) and hn["fallback_count"] == h["fallback_count"]
     assert (hn["msg"] == d["msg"].cpu().numpy()).all() and (hn["iters"] == d["iters"].cpu().numpy()).all()
+
+
+def test_fallback_same_decoder_host_pipeline(gpu):
+    """One layered decoder as both the primary (8 iterations) and the fallback:
+    on host memory each chunk's two passes stay on that chunk's stream and
+    workspace (2800 normal frames, nine chunks on two streams); the results
+    and the count equal the device call's."""
+    code = g.LdpcCode.dvb_t2_normal(g.CodeRate.Rate2_3)
+    dec = g.LdpcDecoder(code, algorithm=g.ALGO_SPA_FAST, schedule=g.SCHED_LAYERED, msg_dtype=g.MSG_F16)
+    F = 2800
+    s2 = np.array([g.sigma2_from_ebn0(2.0 + 0.2 * (f % 6), code.rate()) for f in range(F)])
+    _, _, llr = g.awgn_frames(code, 44, 0, F, s2, device=gpu, want_info=False, want_cw=False)
+    d = dec.decode_with_fallback(dec, llr, 8, 50)
+    torch.cuda.synchronize()
+    assert 0 < int(d["fallback_count"][0]) < F
+    h = dec.decode_with_fallback(dec, llr.cpu().pin_memory(), 8, 50)
+    assert h["fallback_count"] == int(d["fallback_count"][0])
+    for k in ("msg", "iters", "conv", "synd_ok"):
+        assert torch.equal(h[k], d[k].cpu()), k
